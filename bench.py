@@ -1,0 +1,408 @@
+"""Benchmark of the FFT hot path on B200.
+
+Workload (the configuration the headline metric is quoted on): 1D real
+transforms in FP32 — R2C FORWARD then C2R INVERSE — at N=3000 (2^3*3*5^3) and
+N=4096, batch 4096 each.  Input: seeded Gaussian noise (sigma=1) plus three
+sinusoids at random bins with amplitudes in [0.1, 10].  One step = the four
+launches R2C(3000), C2R(3000), R2C(4096), C2R(4096) over the full batches.
+
+Metric: FFT GFLOP/s with 5*N*log2(N) flops per transform (also for R2C/C2R),
+whole job (all ranks).  `value` is timed with inputs resident in HBM and L2
+flushed (256 MiB write) between steps; `e2e` goes through the C ABI's aclTensor
+entry points with pinned host buffers, H2D of the inputs and D2H of the
+round-trip results inside the timed region.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun every rank runs an independent replica (the transforms shard
+with no exchange); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SIZES = (3000, 4096)
+BATCH = 4096
+METRIC = "FFT GFLOP/s (5N*log2N per transform), R2C+C2R round trip"
+WORKLOAD = "1D R2C FORWARD + C2R INVERSE, FP32, N=3000 and N=4096, batch 4096 each"
+
+
+def flops_per_transform(n: int) -> float:
+    return 5.0 * n * math.log2(n)
+
+
+def step_flops() -> float:
+    return sum(2 * BATCH * flops_per_transform(n) for n in SIZES)
+
+
+def algorithmic_bytes(n: int) -> int:
+    """One read of the input and one write of the output, per launch (R2C and C2R alike)."""
+    return BATCH * (4 * n + 8 * (n // 2 + 1))
+
+
+def make_signal(n: int, rows: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((rows, n))
+    t = np.arange(n)
+    for _ in range(3):
+        k = rng.integers(1, n // 2, size=(rows, 1))
+        a = rng.uniform(0.1, 10.0, size=(rows, 1))
+        ph = rng.uniform(0, 2 * np.pi, size=(rows, 1))
+        x += a * np.cos(2 * np.pi * k * t / n + ph)
+    return x.astype(np.float32)
+
+
+# ----------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic() -> dict | None:
+    path = os.path.join(ROOT, "profiles", "r2c_c2r_roundtrip_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+# ----------------------------------------------------------------------------------- CPU baseline
+def cpu_baseline(budget_s: float = 10.0) -> dict:
+    """FP64 host FFT (the oracle port: scipy pocketfft) on a bounded sample of the workload."""
+    import scipy.fft as sfft
+
+    cores = os.cpu_count() or 1
+    rows = 256
+    xs = {n: make_signal(n, rows, 100 + n).astype(np.float64) for n in SIZES}
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        for n in SIZES:
+            X = sfft.rfft(xs[n], axis=-1, workers=cores)
+            sfft.irfft(X, n=n, axis=-1, workers=cores)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or reps >= 2000:
+            break
+    fl = reps * sum(2 * rows * flops_per_transform(n) for n in SIZES)
+    return {"value": fl / el / 1e9, "unit": "GFLOP/s", "cores": cores, "kind": "port",
+            "sample": f"{reps} x (rfft+irfft of {rows} rows at N=3000 and N=4096), complex128/float64 "
+                      f"scipy.fft workers={cores}, {el:.1f} s"}
+
+
+# ----------------------------------------------------------------------------------- distributed
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------------------- reference arm
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import scipy.fft as sfft
+
+    cores = os.cpu_count() or 1
+    rows = 256
+    xs = {n: make_signal(n, rows, 100 + n).astype(np.float64) for n in SIZES}
+
+    def one():
+        for n in SIZES:
+            X = sfft.rfft(xs[n], axis=-1, workers=cores)
+            sfft.irfft(X, n=n, axis=-1, workers=cores)
+
+    for _ in range(args.warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one()
+    el = time.perf_counter() - t0
+    fl = args.steps * sum(2 * rows * flops_per_transform(n) for n in SIZES)
+    v = fl / el / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Gaussian + 3 sinusoids)",
+        "config": {"workload": WORKLOAD + f"; each step a bounded sample of {rows} rows per length",
+                   "batch": rows, "sizes": list(SIZES)},
+        "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": cores, "kind": "port",
+                         "sample": f"{rows} rows per length per step; the reference's FFT runs only on an "
+                                   f"Ascend NPU, so its CPU stand-in is the FP64 host FFT (scipy pocketfft)"},
+        "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------- our arm
+def run_ours(args, world, rank, local):
+    import ctypes
+
+    import torch
+
+    from sip_b200 import fft
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    fft.load_library()
+    stream = torch.cuda.Stream(device=dev)
+    R2C, C2R, FWD, INV = fft.ASCEND_FFT_R2C, fft.ASCEND_FFT_C2R, fft.ASCEND_FFT_FORWARD, fft.ASCEND_FFT_INVERSE
+
+    plans, bufs = [], []
+    host_in, host_out = {}, {}
+    for n in SIZES:
+        x = make_signal(n, BATCH, seed=1000 * rank + n)
+        xd = torch.from_numpy(x).to(dev)
+        X = torch.empty((BATCH, n // 2 + 1), dtype=torch.complex64, device=dev)
+        y = torch.empty_like(xd)
+        f = fft.FftPlan([n], R2C, FWD, BATCH, stream=stream)
+        g = fft.FftPlan([n], C2R, INV, BATCH, stream=stream)
+        plans.append((n, f, g))
+        bufs.append((xd, X, y))
+        host_in[n] = torch.from_numpy(x).pin_memory()
+        host_out[n] = torch.empty_like(host_in[n]).pin_memory()
+
+    # Tensor descriptors are built once, as a caller of the C ABI would.
+    descs = []
+    for (n, f, g), (xd, X, y) in zip(plans, bufs):
+        descs.append((fft.AclTensor.from_torch(xd), fft.AclTensor.from_torch(X), fft.AclTensor.from_torch(y)))
+    lib = fft.load_library()
+
+    def launch_step(events=None):
+        i = 0
+        for (n, f, g), (ax, aX, ay) in zip(plans, descs):
+            if events is not None:
+                events[i].record(stream)
+            st = lib.asdFftExecR2C(f.handle, ax.ptr, aX.ptr)
+            if events is not None:
+                events[i + 1].record(stream)
+            st2 = lib.asdFftExecC2R(g.handle, aX.ptr, ay.ptr)
+            if st or st2:
+                raise RuntimeError(f"exec failed: {st} {st2}")
+            i += 2
+        if events is not None:
+            events[i].record(stream)
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    # ---------------- accuracy of the round trip on this data
+    with torch.cuda.stream(stream):
+        launch_step()
+    stream.synchronize()
+    acc = {}
+    from oracle import oracle as _oracle  # checker only
+
+    for (n, f, g), (xd, X, y) in zip(plans, bufs):
+        xr = xd[:256].double().cpu().numpy()
+        yr = y[:256].double().cpu().numpy() / n
+        acc[str(n)] = {"round_trip_rel_l2": _oracle.rel_l2(yr, xr),
+                       "r2c_rel_l2_vs_fp64": _oracle.rel_l2(X[:64].cpu().numpy(), _oracle.r2c(xr[:64], True)),
+                       "bound": _oracle.tolerance(n)}
+
+    # ---------------- device-resident timing
+    for _ in range(max(3, args.warmup)):
+        flush.fill_(1.0)
+        with torch.cuda.stream(stream):
+            launch_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+    nlaunch = 2 * len(SIZES)
+    step_ms, launch_ms = [], [[] for _ in range(nlaunch)]
+    sampler = ClockSampler(local) if rank == 0 or True else None
+    sampler.start()
+    time.sleep(0.3)
+    for _ in range(args.steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(nlaunch + 1)]
+        flush.fill_(1.0)  # L2 flush between timed steps, outside the events
+        with torch.cuda.stream(stream):
+            launch_step(ev)
+        stream.synchronize()
+        step_ms.append(ev[0].elapsed_time(ev[-1]))
+        for i in range(nlaunch):
+            launch_ms[i].append(ev[i].elapsed_time(ev[i + 1]))
+    clocks = sampler.stop()
+    torch.cuda.synchronize()
+    total_s = sum(step_ms) / 1e3
+    total_s = max_over_ranks(total_s, world)
+    flops = step_flops() * args.steps * world
+    value = flops / total_s / 1e9
+
+    # roofline of the dominant kernel (every launch of the step is the tile kernel)
+    peak, peak_kind = measured_peak_hbm()
+    alg_bytes = sum(algorithmic_bytes(n) for n in SIZES) * 2  # R2C + C2R per length
+    kern_s = sum(sum(l) for l in launch_ms) / 1e3 / args.steps  # per step
+    achieved = alg_bytes / kern_s / 1e9
+    per_launch = {}
+    for i, (n, _, _) in enumerate(plans):
+        for j, kind in enumerate(("r2c", "c2r")):
+            ms = statistics.median(launch_ms[2 * i + j])
+            per_launch[f"{kind}_{n}"] = {"ms": ms, "GBps": algorithmic_bytes(n) / (ms / 1e3) / 1e9}
+    traffic = profiled_traffic()
+
+    # ---------------- end to end through the C ABI with host buffers
+    e2e_ms = []
+    h2d = sum(host_in[n].numel() * 4 for n in SIZES)
+    d2h = sum(host_out[n].numel() * 4 for n in SIZES)
+    for it in range(args.warmup + args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for (n, f, g), (xd, X, y) in zip(plans, bufs):
+                xd.copy_(host_in[n], non_blocking=True)
+            launch_step()
+            for (n, f, g), (xd, X, y) in zip(plans, bufs):
+                host_out[n].copy_(y, non_blocking=True)
+            e1.record(stream)
+        stream.synchronize()
+        if it >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_s = max_over_ranks(sum(e2e_ms) / 1e3, world)
+    e2e_value = step_flops() * args.steps * world / e2e_s / 1e9
+
+    launches_per_step = sum(f.launches() + g.launches() for _, f, g in plans)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_s / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Gaussian noise + 3 sinusoids, amplitudes U[0.1,10])",
+            "config": {"workload": WORKLOAD, "batch": BATCH, "sizes": list(SIZES),
+                       "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": (traffic or {}).get("traffic_bytes_per_step"),
+                         "algorithmic_bytes_per_step": alg_bytes, "kernel": "sipfft::tile_fft_kernel",
+                         "per_launch": per_launch},
+            "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_s / args.steps * 1e3},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clocks,
+            "accuracy": acc,
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+    for d in descs:
+        for t in d:
+            t.close()
+    for _, f, g in plans:
+        f.close()
+        g.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,105 @@
+// Stand-alone R2C post-twiddle and C2R pre-twiddle kernels.  They are used
+// only by real transforms too long for one CTA (the fused single-CTA kernels
+// do the same arithmetic inside fft_tile.cu).  The maths follows the
+// reference's even-length path (core/fft/fftcore/include/fftcore/fft_r2c_core.h:21-24,
+// A/B tables in fft_core_common_func.cpp:569-673), written as the split
+// X[k] = E[k] + w^k O[k] with E, O recovered from the packed spectrum Z.
+#include "codelets.cuh"
+#include "sipfft_internal.h"
+
+namespace sipfft {
+
+template <bool FWD>
+__device__ __forceinline__ float2 tw2(const float2 *lo, const float2 *hi, int log2l, int64_t m)
+{
+    const int64_t mask = (int64_t(1) << log2l) - 1;
+    return dir<FWD>(cmul(__ldg(lo + (m & mask)), __ldg(hi + (m >> log2l))));
+}
+
+// Z: [rows][m] packed spectrum of z[j] = x[2j] + i x[2j+1]; X: [rows][m+1]
+template <bool FWD>
+__global__ void r2c_post_kernel(const float2 *__restrict__ z, float2 *__restrict__ x, int64_t m, int64_t zdist,
+                                int64_t xdist, const float2 *lo, const float2 *hi, int log2l)
+{
+    const int64_t row = blockIdx.y;
+    const float2 *zr = z + row * zdist;
+    float2 *xr = x + row * xdist;
+    for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; 2 * k <= m;
+         k += int64_t(gridDim.x) * blockDim.x) {
+        const float2 zk = zr[k];
+        const float2 zm = cconj(zr[k == 0 ? 0 : m - k]);
+        const float2 e = cscale(cadd(zk, zm), 0.5f);
+        const float2 t = csub(zk, zm);
+        const float2 od = make_float2(0.5f * t.y, -0.5f * t.x);
+        const float2 wo = cmul(tw2<FWD>(lo, hi, log2l, k), od);
+        xr[k] = cadd(e, wo);
+        if (2 * k != m) xr[m - k] = cconj(csub(e, wo));
+    }
+}
+
+// X: [rows][m+1] half spectrum; Z: [rows][m] packed input of the m-point FFT
+template <bool FWD>
+__global__ void c2r_pre_kernel(const float2 *__restrict__ x, float2 *__restrict__ z, int64_t m, int64_t xdist,
+                               int64_t zdist, const float2 *lo, const float2 *hi, int log2l)
+{
+    const int64_t row = blockIdx.y;
+    const float2 *xr = x + row * xdist;
+    float2 *zr = z + row * zdist;
+    for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; 2 * k <= m;
+         k += int64_t(gridDim.x) * blockDim.x) {
+        float2 xk = xr[k];
+        float2 xm = xr[m - k];
+        if (k == 0) {
+            xk.y = 0.f;
+            xm.y = 0.f;
+        }
+        const float2 e = cadd(xk, cconj(xm));
+        const float2 od = cmul(csub(xk, cconj(xm)), tw2<FWD>(lo, hi, log2l, k));
+        zr[k] = make_float2(e.x - od.y, e.y + od.x);
+        if (k != 0 && 2 * k != m) zr[m - k] = make_float2(e.x + od.y, -e.y + od.x);
+    }
+}
+
+namespace {
+dim3 aux_grid(int64_t rows, int64_t m)
+{
+    const int64_t pairs = m / 2 + 1;
+    int64_t gx = (pairs + 255) / 256;
+    if (gx > 1024) gx = 1024;
+    return dim3(static_cast<unsigned>(gx), static_cast<unsigned>(rows), 1);
+}
+}  // namespace
+
+cudaError_t launch_r2c_post(const float2 *z, float2 *x, int64_t rows, int64_t m, int64_t zdist, int64_t xdist,
+                            const float2 *lo, const float2 *hi, int log2l, bool forward, cudaStream_t st)
+{
+    for (int64_t r0 = 0; r0 < rows; r0 += 65535) {
+        const int64_t nr = rows - r0 < 65535 ? rows - r0 : 65535;
+        const dim3 g = aux_grid(nr, m);
+        if (forward)
+            r2c_post_kernel<true><<<g, 256, 0, st>>>(z + r0 * zdist, x + r0 * xdist, m, zdist, xdist, lo, hi, log2l);
+        else
+            r2c_post_kernel<false><<<g, 256, 0, st>>>(z + r0 * zdist, x + r0 * xdist, m, zdist, xdist, lo, hi, log2l);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_c2r_pre(const float2 *x, float2 *z, int64_t rows, int64_t m, int64_t xdist, int64_t zdist,
+                           const float2 *lo, const float2 *hi, int log2l, bool forward, cudaStream_t st)
+{
+    for (int64_t r0 = 0; r0 < rows; r0 += 65535) {
+        const int64_t nr = rows - r0 < 65535 ? rows - r0 : 65535;
+        const dim3 g = aux_grid(nr, m);
+        if (forward)
+            c2r_pre_kernel<true><<<g, 256, 0, st>>>(x + r0 * xdist, z + r0 * zdist, m, xdist, zdist, lo, hi, log2l);
+        else
+            c2r_pre_kernel<false><<<g, 256, 0, st>>>(x + r0 * xdist, z + r0 * zdist, m, xdist, zdist, lo, hi, log2l);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace sipfft

@@ -1,0 +1,329 @@
+// sm_100a tile FFT kernel: shared-memory-resident mixed-radix Stockham.
+//
+// One CTA owns `tb` transforms of length n (or `tb` columns of a multi-pass
+// Stockham pass).  Phases:
+//   1. load  — HBM -> shared memory, coalesced along whichever axis is
+//              contiguous in HBM (rows: along the transform; columns: across
+//              transforms), with R2C/C2R packing and pass twiddles applied;
+//   2. stages — for each radix R: every thread gathers its butterflies'
+//              R inputs into registers, applies the stage twiddles, runs the
+//              register codelet, barrier, scatters the outputs (Stockham
+//              autosort, so no digit reversal pass);
+//   3. store — shared memory -> HBM with the R2C post-twiddle or the
+//              transposed (column) layout of the next axis / next pass.
+// HBM traffic per launch is one read and one write of the tile.
+// The shared-memory row index is padded (i + i/16) so that the strided
+// scatter of the early stages and the column-tile loads are bank-conflict
+// free for 8-byte elements.
+#include "codelets.cuh"
+#include "fft_tile.cuh"
+#include "sipfft_internal.h"
+
+namespace sipfft {
+
+__device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+
+__device__ __forceinline__ int64_t col_base(const Addr &a, int64_t o, int64_t c)
+{
+    int64_t x = o * a.dist + c * a.cstride;
+    if (a.cblock) x += (c / a.cblock) * a.cjump;
+    return x;
+}
+
+// Register budget of one stage: NB butterflies of radix R per thread.
+template <int R, int MAXE>
+constexpr int nb_for() { return (MAXE + R - 1) / R; }
+template <int MAXE>
+constexpr int maxv_for()
+{
+    constexpr int r[] = {2, 3, 4, 5, 7, 8, 11, 13, 16};
+    int m = 0;
+    for (int x : r) m = m > ((MAXE + x - 1) / x) * x ? m : ((MAXE + x - 1) / x) * x;
+    return m;
+}
+
+// Gather the R inputs of each of this thread's butterflies, apply the stage
+// twiddles and run the codelet; results stay in v until after the barrier.
+template <int R, int MAXE, bool FWD>
+__device__ __forceinline__ void stage_read(float2 *v, const float2 *row, int n, int ns, int tstep, int lane, int tpt,
+                                           bool active, const float2 *__restrict__ tw)
+{
+    constexpr int NB = nb_for<R, MAXE>();
+    const int nbf = n / R;
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        const int j = lane + b * tpt;
+        if (active && j < nbf) {
+#pragma unroll
+            for (int r = 0; r < R; r++) v[b * R + r] = row[pad(j + r * nbf)];
+            if (ns > 1) {
+                const int step = (j % ns) * tstep;
+#pragma unroll
+                for (int r = 1; r < R; r++) v[b * R + r] = cmul(v[b * R + r], dir<FWD>(__ldg(tw + r * step)));
+            }
+            dft<R, FWD>(v + b * R);
+        }
+    }
+}
+
+// Scatter the butterfly outputs to their Stockham positions.
+template <int R, int MAXE>
+__device__ __forceinline__ void stage_write(const float2 *v, float2 *row, int n, int ns, int lane, int tpt,
+                                            bool active)
+{
+    constexpr int NB = nb_for<R, MAXE>();
+    const int nbf = n / R;
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        const int j = lane + b * tpt;
+        if (active && j < nbf) {
+            const int k = j % ns;
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; r++) row[pad(base + r * ns)] = v[b * R + r];
+        }
+    }
+}
+
+#define SIPFFT_RADIX_CASES(X) X(2) X(3) X(4) X(5) X(7) X(8) X(11) X(13) X(16)
+
+// One register array is shared by all radices so that only one set of
+// butterfly values is live across each stage barrier.
+template <int MAXE, bool FWD>
+__device__ __forceinline__ void run_stages(float2 *row, const TileDesc &d, int lane, bool active)
+{
+    float2 v[maxv_for<MAXE>()];
+#pragma unroll 1
+    for (int s = 0; s < d.nstages; s++) {
+        const int ns = d.ns[s], ts = d.tstep[s], R = d.radix[s];
+        switch (R) {
+#define SIPFFT_READ(RR) \
+    case RR: stage_read<RR, MAXE, FWD>(v, row, d.n, ns, ts, lane, d.tpt, active, d.tw); break;
+            SIPFFT_RADIX_CASES(SIPFFT_READ)
+#undef SIPFFT_READ
+            default: break;  // the planner only emits the radices above
+        }
+        __syncthreads();
+        switch (R) {
+#define SIPFFT_WRITE(RR) \
+    case RR: stage_write<RR, MAXE>(v, row, d.n, ns, lane, d.tpt, active); break;
+            SIPFFT_RADIX_CASES(SIPFFT_WRITE)
+#undef SIPFFT_WRITE
+            default: break;
+        }
+        __syncthreads();
+    }
+}
+
+template <bool FWD>
+__device__ __forceinline__ float2 pass_twiddle(const TileDesc &d, int64_t e, int64_t kc)
+{
+    const int64_t m = e * kc * d.g_step;
+    const int64_t mask = (int64_t(1) << d.g_log2l) - 1;
+    const float2 w = cmul(__ldg(d.g_lo + (m & mask)), __ldg(d.g_hi + (m >> d.g_log2l)));
+    return dir<FWD>(w);
+}
+
+// ------------------------------------------------------------------------------------ load
+template <bool FWD>
+__device__ __forceinline__ void load_tile(const TileDesc &d, float2 *sm, int64_t o, int64_t c0, int ntr)
+{
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int n = d.n, P = d.pitch;
+    const int io = d.io;
+    if (io == IO_C2R_PACKED) {
+        // pairs (k, n-k) of the half spectrum -> packed n-point input
+        const int l = tid / d.tpt, lane = tid % d.tpt;
+        if (l >= ntr) return;
+        const float2 *x = static_cast<const float2 *>(d.in) + col_base(d.in_a, o, c0 + l);
+        float2 *row = sm + l * P;
+        for (int k = lane; 2 * k <= n; k += d.tpt) {
+            float2 xk = x[k];
+            float2 xm = x[n - k];
+            if (k == 0) {
+                xk.y = 0.f;
+                xm.y = 0.f;
+            }
+            const float2 e = cadd(xk, cconj(xm));
+            const float2 w = dir<FWD>(__ldg(d.tw + k));
+            const float2 od = cmul(csub(xk, cconj(xm)), w);
+            // Z[k] = e + i*od ; Z[n-k] = conj(e) + i*conj(od)
+            row[pad(k)] = make_float2(e.x - od.y, e.y + od.x);
+            if (k != 0 && 2 * k != n) row[pad(n - k)] = make_float2(e.x + od.y, -e.y + od.x);
+        }
+        return;
+    }
+    if (io == IO_C2R_FULL) {
+        const int l = tid / d.tpt, lane = tid % d.tpt;
+        if (l >= ntr) return;
+        const float2 *x = static_cast<const float2 *>(d.in) + col_base(d.in_a, o, c0 + l);
+        float2 *row = sm + l * P;
+        for (int k = lane; 2 * k <= n; k += d.tpt) {
+            float2 xk = x[k];
+            if (k == 0) xk.y = 0.f;
+            row[pad(k)] = xk;
+            if (k != 0) row[pad(n - k)] = cconj(xk);
+        }
+        return;
+    }
+    // element-wise kinds: C2C, R2C_PACKED (float pairs), R2C_FULL (floats)
+    const bool contiguous = d.in_a.estride == 1;
+    int l, e0, estep;
+    if (contiguous) {
+        l = tid / d.tpt;
+        e0 = tid % d.tpt;
+        estep = d.tpt;
+    } else {
+        l = tid % d.tb;
+        e0 = tid / d.tb;
+        estep = bd / d.tb;
+    }
+    if (l >= ntr) return;
+    const int64_t base = col_base(d.in_a, o, c0 + l);
+    const int64_t es = d.in_a.estride;
+    float2 *row = sm + l * P;
+    if (io == IO_R2C_FULL) {
+        const float *x = static_cast<const float *>(d.in) + base;
+        for (int e = e0; e < n; e += estep) row[pad(e)] = make_float2(x[e * es], 0.f);
+        return;
+    }
+    const float2 *x = static_cast<const float2 *>(d.in) + base;
+    if (d.g_twiddle) {
+        const int64_t kc = (c0 + l) % d.g_ns;
+        for (int e = e0; e < n; e += estep) row[pad(e)] = cmul(x[e * es], pass_twiddle<FWD>(d, e, kc));
+    } else {
+        for (int e = e0; e < n; e += estep) row[pad(e)] = x[e * es];
+    }
+}
+
+// ------------------------------------------------------------------------------------ store
+template <bool FWD>
+__device__ __forceinline__ void store_tile(const TileDesc &d, const float2 *sm, int64_t o, int64_t c0, int ntr)
+{
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int n = d.n, P = d.pitch;
+    const int io = d.io;
+    if (io == IO_R2C_PACKED) {
+        const int l = tid / d.tpt, lane = tid % d.tpt;
+        if (l >= ntr) return;
+        float2 *y = static_cast<float2 *>(d.out) + col_base(d.out_a, o, c0 + l);
+        const float2 *row = sm + l * P;
+        for (int k = lane; 2 * k <= n; k += d.tpt) {
+            const float2 zk = row[pad(k)];
+            const float2 zm = cconj(row[pad(k == 0 ? 0 : n - k)]);
+            const float2 e = cscale(cadd(zk, zm), 0.5f);
+            const float2 t = csub(zk, zm);
+            const float2 od = make_float2(0.5f * t.y, -0.5f * t.x);  // -i/2 * t
+            const float2 wo = cmul(dir<FWD>(__ldg(d.tw + k)), od);
+            y[k] = cadd(e, wo);
+            if (2 * k != n) y[n - k] = cconj(csub(e, wo));
+        }
+        return;
+    }
+    const bool contiguous = d.out_a.estride == 1;
+    int l, e0, estep;
+    if (contiguous) {
+        l = tid / d.tpt;
+        e0 = tid % d.tpt;
+        estep = d.tpt;
+    } else {
+        l = tid % d.tb;
+        e0 = tid / d.tb;
+        estep = bd / d.tb;
+    }
+    if (l >= ntr) return;
+    const int64_t base = col_base(d.out_a, o, c0 + l);
+    const int64_t es = d.out_a.estride;
+    const float2 *row = sm + l * P;
+    if (io == IO_C2R_FULL) {
+        float *y = static_cast<float *>(d.out) + base;
+        for (int e = e0; e < n; e += estep) y[e * es] = row[pad(e)].x;
+        return;
+    }
+    const int count = (io == IO_R2C_FULL) ? n / 2 + 1 : n;
+    float2 *y = static_cast<float2 *>(d.out) + base;
+    for (int e = e0; e < count; e += estep) y[e * es] = row[pad(e)];
+}
+
+template <int MAXE, bool FWD>
+__global__ void __launch_bounds__(512, 1) tile_fft_kernel(const __grid_constant__ TileDesc d)
+{
+    extern __shared__ float2 sm[];
+    const int tid = threadIdx.x;
+    int l, lane;
+    if (d.xfast) {
+        l = tid % d.tb;
+        lane = tid / d.tb;
+    } else {
+        l = tid / d.tpt;
+        lane = tid % d.tpt;
+    }
+    for (int64_t g = blockIdx.x; g < d.num_tiles; g += gridDim.x) {
+        const int64_t o = g / d.tiles_per_outer;
+        const int64_t c0 = (g % d.tiles_per_outer) * d.tb;
+        const int64_t left = d.n_cols - c0;
+        const int ntr = left < d.tb ? static_cast<int>(left) : d.tb;
+        load_tile<FWD>(d, sm, o, c0, ntr);
+        __syncthreads();
+        run_stages<MAXE, FWD>(sm + l * d.pitch, d, lane, l < ntr);
+        store_tile<FWD>(d, sm, o, c0, ntr);
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------------ twiddles
+// t[m] = exp(-2 pi i * ((m * mult) mod denom) / denom), evaluated in FP64 and
+// rounded once to FP32 (the reference builds its tables the same way on the
+// host: core/fft/fftcore/fft_core_common_func.cpp:214-232).
+__global__ void twiddle_kernel(float2 *t, int64_t count, int64_t denom, int64_t mult)
+{
+    for (int64_t m = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; m < count;
+         m += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t idx = (m * mult) % denom;
+        double s, c;
+        sincospi(2.0 * static_cast<double>(idx) / static_cast<double>(denom), &s, &c);
+        t[m] = make_float2(static_cast<float>(c), static_cast<float>(-s));
+    }
+}
+
+// ------------------------------------------------------------------------------------ host side
+namespace {
+template <int MAXE, bool FWD>
+cudaError_t launch_one(const TileDesc &d, int grid, int block, size_t smem, cudaStream_t st)
+{
+    static bool configured = false;  // attribute is per function; setting it twice is harmless
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(tile_fft_kernel<MAXE, FWD>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBytes);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    tile_fft_kernel<MAXE, FWD><<<grid, block, smem, st>>>(d);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_tile(const TileDesc &d, int maxe, bool forward, int grid, cudaStream_t st)
+{
+    const int block = d.tb * d.tpt;
+    const size_t smem = static_cast<size_t>(d.tb) * d.pitch * sizeof(float2);
+    if (block <= 0 || block > 512 || smem > static_cast<size_t>(kMaxSmemBytes) || grid <= 0)
+        return cudaErrorInvalidConfiguration;
+    if (maxe <= 8) return forward ? launch_one<8, true>(d, grid, block, smem, st)
+                                  : launch_one<8, false>(d, grid, block, smem, st);
+    if (maxe <= 16) return forward ? launch_one<16, true>(d, grid, block, smem, st)
+                                   : launch_one<16, false>(d, grid, block, smem, st);
+    return forward ? launch_one<32, true>(d, grid, block, smem, st) : launch_one<32, false>(d, grid, block, smem, st);
+}
+
+cudaError_t fill_twiddles(float2 *t, int64_t count, int64_t denom, int64_t mult, cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    const int block = 256;
+    int64_t grid = (count + block - 1) / block;
+    if (grid > 4096) grid = 4096;
+    twiddle_kernel<<<static_cast<int>(grid), block, 0, st>>>(t, count, denom, mult);
+    return cudaGetLastError();
+}
+
+}  // namespace sipfft

@@ -1,0 +1,73 @@
+// Kernel-side description of one FFT launch ("tile kernel").
+//
+// Every device step of a plan is one launch of the tile kernel: a CTA loads a
+// tile of `tb` transforms (or of `tb` columns of one Stockham pass) from HBM
+// into shared memory, runs a mixed-radix Stockham FFT of length `n` on each
+// row held in shared memory (register codelets, one barrier pair per stage),
+// and stores the tile back.  Pre/post-processing that the reference runs as
+// separate GM passes (R2C/C2R pack twiddles: core/fft/fftcore/fft_r2c_core.cpp,
+// fft_c2r_core.cpp; inter-stage twiddles of the large-N cores:
+// fft_core_n.cpp, fft_core_mix_base.cpp) and the axis transposes of the
+// multi-dimensional plans (fftoperation/transpose.cpp) are folded into the
+// load and store phases of this kernel.
+#pragma once
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+namespace sipfft {
+
+constexpr int kMaxStages = 16;
+
+enum IoKind : int {
+    IO_C2C = 0,         // complex in, complex out
+    IO_R2C_PACKED = 1,  // even real length 2n read as n complex pairs; n-point FFT; post-twiddle to n+1 bins
+    IO_C2R_PACKED = 2,  // n+1 bins; pre-twiddle to n complex; n-point FFT; written as 2n reals
+    IO_R2C_FULL = 3,    // odd real length n, zero imaginary part; n-point FFT; bins 0..n/2
+    IO_C2R_FULL = 4,    // bins 0..n/2 of odd n, Hermitian extension; n-point FFT; real part
+};
+
+// Address of element e of transform (outer o, column c):
+//   o*dist + c*cstride + (cblock ? (c / cblock) * cjump : 0) + e*estride
+// in units of the array's element type (float2 for complex and for packed
+// real rows, float for the real side of the FULL kinds).
+struct Addr {
+    int64_t dist;
+    int64_t cstride;
+    int64_t estride;
+    int64_t cblock;  // 0 = no block jump
+    int64_t cjump;
+};
+
+struct TileDesc {
+    const void *in;
+    void *out;
+    int n;          // FFT length held in shared memory (complex points)
+    int io;         // IoKind
+    int nstages;
+    int radix[kMaxStages];
+    int ns[kMaxStages];      // product of the radices of the earlier stages
+    int tstep[kMaxStages];   // twiddle table index step: (n / (ns * radix)) * tw_mul
+    int tb;         // transforms (columns) per tile
+    int tpt;        // threads per transform
+    int pitch;      // shared-memory floats2 per transform (padded)
+    int xfast;      // thread mapping: 1 = transform index fastest (column tiles)
+    int64_t n_outer;
+    int64_t n_cols;
+    int64_t tiles_per_outer;
+    int64_t num_tiles;
+    Addr in_a;
+    Addr out_a;
+    const float2 *tw;   // exp(-2 pi i m / (n * tw_mul)), m < n * tw_mul
+    int tw_mul;
+    // Input twiddle of a multi-pass Stockham pass over a length-F transform:
+    // element r of column c is multiplied by W_F^(r * (c mod g_ns) * (F / (g_ns * n))),
+    // read from a two-level table W_F^m = lo[m & (L-1)] * hi[m >> log2 L].
+    int g_twiddle;
+    int g_log2l;
+    int64_t g_ns;
+    int64_t g_step;    // F / (g_ns * n)
+    const float2 *g_lo;
+    const float2 *g_hi;
+};
+
+}  // namespace sipfft

@@ -1,0 +1,519 @@
+// FFT planner: turns a reference-style plan (type, direction, sizes, batch,
+// vertical/horizontal) into a list of tile-kernel launches.
+//
+// Reference counterpart: core/fft/fft_api.cpp — addFFTSteps (485-499),
+// getCore (383-432), init2DSteps (527-602), init3DSteps (604-697) and the
+// per-core radix tables (fft_core_b.cpp:126-168, fft_core_n.cpp:206-265,
+// fft_core_common_func.cpp:675-826).  The reference chooses one of ~16 core
+// families and inserts explicit Transpose steps between axes; here every axis
+// is one launch of the same tile kernel whose load/store addressing walks the
+// axis in place (no transpose steps), and transforms longer than one CTA's
+// shared memory become a short sequence of Stockham passes whose butterflies
+// are shared-memory FFTs (2 passes up to 2^18 complex points, 3 up to 2^27).
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <sstream>
+
+#include "sipfft_internal.h"
+
+namespace sipfft {
+
+namespace {
+
+constexpr int64_t kMaxRowN = 16384;        // longest single-CTA transform: 512 threads x 32 points
+constexpr int kMaxPassRadix = 2048;        // longest sub-FFT of one multi-pass Stockham pass
+constexpr int kRowThreadsTarget = 256;     // threads per CTA for batched rows
+constexpr int kRowSmemTarget = 64 * 1024;  // keep >= 3 CTAs per SM for short rows
+constexpr int kColTile = 16;               // columns per tile: 16 x 8 B = one 128-byte line
+constexpr int kMaxThreads = 512;           // launch bound of the tile kernel (keeps 128 registers/thread)
+const int kRadices[] = {16, 13, 11, 8, 7, 5, 4, 3, 2};
+
+int padded(int i) { return i + (i >> 4); }
+
+int pitch_for(int n)
+{
+    int p = (n > 0 ? padded(n - 1) + 1 : 1);
+    if ((p & 1) == 0) p += 1;  // odd pitch: column-tile accesses hit distinct banks
+    return p;
+}
+
+int ilog2_ceil(int64_t x)
+{
+    int l = 0;
+    while ((int64_t(1) << l) < x) l++;
+    return l;
+}
+
+struct TileCfg {
+    int maxe = 16, tpt = 1, tb = 1, pitch = 1;
+};
+
+// Threads, transforms per CTA and shared-memory pitch for one tile launch.
+bool choose_cfg(int n, bool column, int64_t ncols, TileCfg &c, std::string &err)
+{
+    if (n < 1 || n > 32768) {
+        err = "transform length out of the single-CTA range";
+        return false;
+    }
+    c.maxe = n <= 4096 ? 16 : 32;
+    c.tpt = std::max(1, (n + c.maxe - 1) / c.maxe);
+    if (c.tpt > kMaxThreads) {
+        err = "too many threads per transform";
+        return false;
+    }
+    c.pitch = pitch_for(n);
+    const int64_t bytes_per = int64_t(c.pitch) * 8;
+    if (column) {
+        c.tb = 0;
+        for (int tb = kColTile; tb >= 1; tb /= 2) {
+            if (tb * c.tpt <= kMaxThreads && tb * bytes_per <= kMaxSmemBytes) {
+                c.tb = tb;
+                break;
+            }
+        }
+    } else {
+        int tb = std::max(1, kRowThreadsTarget / c.tpt);
+        while (tb > 1 && tb * bytes_per > kRowSmemTarget) tb /= 2;
+        if (tb > ncols) tb = static_cast<int>(std::max<int64_t>(1, ncols));
+        while (tb > 1 && tb * c.tpt > kMaxThreads) tb /= 2;
+        c.tb = (bytes_per <= kMaxSmemBytes) ? tb : 0;
+    }
+    if (c.tb == 0) {
+        err = "transform does not fit in shared memory";
+        return false;
+    }
+    return true;
+}
+
+int grid_for(int64_t tiles)
+{
+    const int64_t cap = int64_t(kB200Sms) * 64;
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(tiles, cap)));
+}
+
+void set_stages(TileDesc &d, const std::vector<int> &radices, int n, int tw_mul)
+{
+    d.nstages = static_cast<int>(radices.size());
+    int ns = 1;
+    for (size_t s = 0; s < radices.size(); s++) {
+        d.radix[s] = radices[s];
+        d.ns[s] = ns;
+        d.tstep[s] = (n / (ns * radices[s])) * tw_mul;
+        ns *= radices[s];
+    }
+}
+
+// Split the prime factors of n into `parts` groups with balanced products.
+bool split_passes(int64_t n, int parts, std::vector<int> &out)
+{
+    std::vector<int64_t> primes;
+    int64_t m = n;
+    for (int64_t f = 2; f * f <= m; f++)
+        while (m % f == 0) {
+            primes.push_back(f);
+            m /= f;
+        }
+    if (m > 1) primes.push_back(m);
+    std::sort(primes.rbegin(), primes.rend());
+    std::vector<int64_t> g(parts, 1);
+    for (int64_t p : primes) {
+        auto it = std::min_element(g.begin(), g.end());
+        *it *= p;
+    }
+    out.clear();
+    for (int64_t v : g) {
+        if (v > kMaxPassRadix) return false;
+        out.push_back(static_cast<int>(v));
+    }
+    std::sort(out.rbegin(), out.rend());
+    return true;
+}
+
+struct Builder {
+    Plan &p;
+    bool fwd;
+    int device;
+    explicit Builder(Plan &plan) : p(plan), fwd(plan.forward()), device(plan.device) {}
+
+    std::string err;
+
+    const float2 *table(int64_t count, int64_t denom, int64_t mult = 1)
+    {
+        TablePtr t = get_table(count, denom, mult, device, &err);
+        if (!t) return nullptr;
+        p.tables.push_back(t);
+        return t->ptr;
+    }
+
+    // two-level table for W_F^m, m < F: lo[m & (L-1)] * hi[m >> log2 L]
+    bool table2(int64_t F, const float2 *&lo, const float2 *&hi, int &log2l)
+    {
+        log2l = std::max(1, (ilog2_ceil(F) + 1) / 2);
+        const int64_t L = int64_t(1) << log2l;
+        lo = table(L, F, 1);
+        hi = table((F + L - 1) / L, F, L);
+        return lo && hi;
+    }
+
+    void need_ws(Buf b, size_t bytes)
+    {
+        const int i = b == Buf::kWs0 ? 0 : 1;
+        p.ws_buf_bytes[i] = std::max(p.ws_buf_bytes[i], bytes);
+    }
+
+    // One single-CTA launch over a set of transforms.
+    bool add_tile(int io, int n, int tw_mul, const float2 *tw, bool column, int64_t n_outer, int64_t n_cols,
+                  const Addr &ia, const Addr &oa, Buf src, Buf dst, const std::string &what)
+    {
+        std::vector<int> radices;
+        if (!factor_radices(n, radices)) {
+            err = "length " + std::to_string(n) + " has a prime factor above 13";
+            return false;
+        }
+        TileCfg c;
+        if (!choose_cfg(n, column, n_cols, c, err)) return false;
+        Step s;
+        s.kind = StepKind::kTile;
+        s.forward = fwd;
+        s.src = src;
+        s.dst = dst;
+        s.maxe = c.maxe;
+        s.what = what;
+        TileDesc &d = s.d;
+        d.n = n;
+        d.io = io;
+        set_stages(d, radices, n, tw_mul);
+        d.tb = c.tb;
+        d.tpt = c.tpt;
+        d.pitch = c.pitch;
+        d.xfast = column ? 1 : 0;
+        d.n_outer = n_outer;
+        d.n_cols = n_cols;
+        d.tiles_per_outer = (n_cols + c.tb - 1) / c.tb;
+        d.num_tiles = d.tiles_per_outer * n_outer;
+        d.in_a = ia;
+        d.out_a = oa;
+        d.tw = tw;
+        d.tw_mul = tw_mul;
+        s.grid = grid_for(d.num_tiles);
+        p.steps.push_back(s);
+        return true;
+    }
+
+    Buf other_ws(Buf a, Buf b)
+    {
+        if (a != Buf::kWs0 && b != Buf::kWs0) return Buf::kWs0;
+        if (a != Buf::kWs1 && b != Buf::kWs1) return Buf::kWs1;
+        return Buf::kWs0;
+    }
+
+    // Multi-pass Stockham C2C of length F over `rows` contiguous rows.
+    // src rows have distance in_dist, dst rows out_dist (complex units).
+    bool add_multipass(int64_t F, int64_t rows, int64_t in_dist, int64_t out_dist, Buf src, Buf dst)
+    {
+        std::vector<int> passes;
+        int parts = 2;
+        while (!split_passes(F, parts, passes)) {
+            if (++parts > 6) {
+                err = "length " + std::to_string(F) + " cannot be split into shared-memory passes";
+                return false;
+            }
+        }
+        const float2 *lo = nullptr, *hi = nullptr;
+        int log2l = 0;
+        if (!table2(F, lo, hi, log2l)) return false;
+        Buf cur = src;
+        int64_t cur_dist = in_dist;
+        int64_t ns = 1;
+        for (size_t i = 0; i < passes.size(); i++) {
+            const int rp = passes[i];
+            const bool last = i + 1 == passes.size();
+            Buf nxt = last ? dst : other_ws(cur, dst);
+            const int64_t nxt_dist = last ? out_dist : F;
+            if (!last) need_ws(nxt, size_t(rows) * F * sizeof(float2));
+            const float2 *tw = table(rp, rp);
+            if (!tw) return false;
+            Addr ia{cur_dist, 1, F / rp, 0, 0};
+            Addr oa{nxt_dist, 1, ns, ns, ns * (rp - 1)};
+            std::ostringstream w;
+            w << "pass " << i << " radix " << rp << " of " << F << " (Ns=" << ns << ")";
+            if (!add_tile(IO_C2C, rp, 1, tw, true, rows, F / rp, ia, oa, cur, nxt, w.str())) return false;
+            TileDesc &d = p.steps.back().d;
+            d.g_twiddle = ns > 1 ? 1 : 0;
+            d.g_ns = ns;
+            d.g_step = F / (ns * rp);
+            d.g_lo = lo;
+            d.g_hi = hi;
+            d.g_log2l = log2l;
+            ns *= rp;
+            cur = nxt;
+            cur_dist = nxt_dist;
+        }
+        return true;
+    }
+
+    // C2C along one axis of a contiguous tensor viewed as [outer][n][inner].
+    bool axis_c2c(int64_t n, int64_t outer, int64_t inner, Buf src, Buf dst)
+    {
+        if (n == 1) {
+            // identity along this axis; still move the data when src != dst
+            if (src == dst) return true;
+            return add_copy(outer * inner, src, dst);
+        }
+        std::ostringstream w;
+        w << "C2C axis n=" << n << " outer=" << outer << " inner=" << inner;
+        if (inner == 1) {
+            if (n <= kMaxRowN) {
+                const float2 *tw = table(n, n);
+                if (!tw) return false;
+                Addr a{0, n, 1, 0, 0};
+                return add_tile(IO_C2C, static_cast<int>(n), 1, tw, false, 1, outer, a, a, src, dst, w.str());
+            }
+            return add_multipass(n, outer, n, n, src, dst);
+        }
+        TileCfg c;
+        if (n > 32768 || !choose_cfg(static_cast<int>(n), true, inner, c, err)) {
+            err = "strided axis of length " + std::to_string(n) + " is not supported";
+            return false;
+        }
+        const float2 *tw = table(n, n);
+        if (!tw) return false;
+        Addr a{n * inner, 1, inner, 0, 0};
+        return add_tile(IO_C2C, static_cast<int>(n), 1, tw, true, outer, inner, a, a, src, dst, w.str());
+    }
+
+    // Plain copy expressed as a length-1 transform (keeps one kernel family).
+    bool add_copy(int64_t count, Buf src, Buf dst)
+    {
+        const float2 *tw = table(1, 1);
+        if (!tw) return false;
+        Addr a{0, 1, 1, 0, 0};
+        return add_tile(IO_C2C, 1, 1, tw, false, 1, count, a, a, src, dst, "copy");
+    }
+
+    // R2C along contiguous rows of real length n (output rows of n/2+1 bins).
+    bool rows_r2c(int64_t n, int64_t rows, Buf src, Buf dst)
+    {
+        const int64_t h = n / 2 + 1;
+        std::ostringstream w;
+        w << "R2C rows n=" << n << " rows=" << rows;
+        if (n % 2 == 0 && n / 2 <= kMaxRowN) {
+            const int m = static_cast<int>(n / 2);
+            const float2 *tw = table(n, n);
+            if (!tw) return false;
+            Addr ia{0, m, 1, 0, 0};  // real row viewed as m float pairs
+            Addr oa{0, h, 1, 0, 0};
+            return add_tile(IO_R2C_PACKED, m, 2, tw, false, 1, rows, ia, oa, src, dst, w.str());
+        }
+        if (n % 2 == 1 && n <= kMaxRowN) {
+            const float2 *tw = table(n, n);
+            if (!tw) return false;
+            Addr ia{0, n, 1, 0, 0};
+            Addr oa{0, h, 1, 0, 0};
+            return add_tile(IO_R2C_FULL, static_cast<int>(n), 1, tw, false, 1, rows, ia, oa, src, dst, w.str());
+        }
+        if (n % 2 == 0) {
+            // packed multi-pass FFT of n/2 points into a workspace, then the post-twiddle
+            const int64_t m = n / 2;
+            Buf z = other_ws(src, dst);
+            need_ws(z, size_t(rows) * m * sizeof(float2));
+            if (!add_multipass(m, rows, m, m, src, z)) return false;
+            Step s;
+            s.kind = StepKind::kR2CPost;
+            s.forward = fwd;
+            s.src = z;
+            s.dst = dst;
+            s.rows = rows;
+            s.m = m;
+            s.src_dist = m;
+            s.dst_dist = h;
+            s.what = "R2C post-twiddle n=" + std::to_string(n);
+            if (!table2(n, s.lo, s.hi, s.log2l)) return false;
+            p.steps.push_back(s);
+            return true;
+        }
+        err = "odd real length above " + std::to_string(kMaxRowN) + " is not supported";
+        return false;
+    }
+
+    // C2R along contiguous rows (input rows of n/2+1 bins, output n reals).
+    bool rows_c2r(int64_t n, int64_t rows, Buf src, Buf dst)
+    {
+        const int64_t h = n / 2 + 1;
+        std::ostringstream w;
+        w << "C2R rows n=" << n << " rows=" << rows;
+        if (n % 2 == 0 && n / 2 <= kMaxRowN) {
+            const int m = static_cast<int>(n / 2);
+            const float2 *tw = table(n, n);
+            if (!tw) return false;
+            Addr ia{0, h, 1, 0, 0};
+            Addr oa{0, m, 1, 0, 0};
+            return add_tile(IO_C2R_PACKED, m, 2, tw, false, 1, rows, ia, oa, src, dst, w.str());
+        }
+        if (n % 2 == 1 && n <= kMaxRowN) {
+            const float2 *tw = table(n, n);
+            if (!tw) return false;
+            Addr ia{0, h, 1, 0, 0};
+            Addr oa{0, n, 1, 0, 0};
+            return add_tile(IO_C2R_FULL, static_cast<int>(n), 1, tw, false, 1, rows, ia, oa, src, dst, w.str());
+        }
+        if (n % 2 == 0) {
+            const int64_t m = n / 2;
+            Buf z = other_ws(src, dst);
+            need_ws(z, size_t(rows) * m * sizeof(float2));
+            Step s;
+            s.kind = StepKind::kC2RPre;
+            s.forward = fwd;
+            s.src = src;
+            s.dst = z;
+            s.rows = rows;
+            s.m = m;
+            s.src_dist = h;
+            s.dst_dist = m;
+            s.what = "C2R pre-twiddle n=" + std::to_string(n);
+            if (!table2(n, s.lo, s.hi, s.log2l)) return false;
+            p.steps.push_back(s);
+            return add_multipass(m, rows, m, m, z, dst);
+        }
+        err = "odd real length above " + std::to_string(kMaxRowN) + " is not supported";
+        return false;
+    }
+};
+
+std::string finish(Plan &p, Builder &b, bool ok)
+{
+    if (!ok) {
+        p.steps.clear();
+        return b.err.empty() ? std::string("planning failed") : b.err;
+    }
+    p.ws_bytes = 0;
+    if (p.ws_buf_bytes[0] || p.ws_buf_bytes[1]) {
+        auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+        p.ws_bytes = al(p.ws_buf_bytes[0]) + al(p.ws_buf_bytes[1]);
+    }
+    return std::string();
+}
+
+}  // namespace
+
+bool factor_radices(int64_t n, std::vector<int> &radices)
+{
+    radices.clear();
+    if (n < 1) return false;
+    int64_t m = n;
+    int twos = 0;
+    while (m % 2 == 0) {
+        m /= 2;
+        twos++;
+    }
+    if (twos > 0) {
+        const int s = (twos + 3) / 4;
+        const int base = twos / s, extra = twos % s;
+        for (int i = 0; i < s; i++) radices.push_back(1 << (base + (i < extra ? 1 : 0)));
+    }
+    for (int p : {13, 11, 7, 5, 3}) {
+        while (m % p == 0) {
+            radices.push_back(p);
+            m /= p;
+        }
+    }
+    return m == 1;
+}
+
+bool Plan::forward() const { return direction == 0x10; }
+
+std::string build_plan_1d(Plan &p)
+{
+    Builder b(p);
+    const int64_t n = p.sizes[0];
+    bool ok = false;
+    switch (p.fft_type) {
+        case 0x10:  // C2C
+            ok = p.vertical ? b.axis_c2c(n, 1, p.batch, Buf::kUserIn, Buf::kUserOut)
+                            : b.axis_c2c(n, p.batch, 1, Buf::kUserIn, Buf::kUserOut);
+            break;
+        case 0x12:  // R2C
+            ok = b.rows_r2c(n, p.batch, Buf::kUserIn, Buf::kUserOut);
+            break;
+        case 0x11:  // C2R
+            ok = b.rows_c2r(n, p.batch, Buf::kUserIn, Buf::kUserOut);
+            break;
+        default:
+            b.err = "unsupported transform type";
+    }
+    return finish(p, b, ok);
+}
+
+std::string build_plan_2d(Plan &p)
+{
+    Builder b(p);
+    const int64_t B = p.batch, X = p.sizes[0], Y = p.sizes[1];
+    const int64_t Yh = Y / 2 + 1;
+    bool ok = false;
+    switch (p.fft_type) {
+        case 0x10:
+            ok = b.axis_c2c(Y, B * X, 1, Buf::kUserIn, Buf::kUserOut) &&
+                 b.axis_c2c(X, B, Y, Buf::kUserOut, Buf::kUserOut);
+            break;
+        case 0x12:
+            ok = b.rows_r2c(Y, B * X, Buf::kUserIn, Buf::kUserOut) &&
+                 b.axis_c2c(X, B, Yh, Buf::kUserOut, Buf::kUserOut);
+            break;
+        case 0x11:
+            b.need_ws(Buf::kWs0, size_t(B) * X * Yh * sizeof(float2));
+            ok = b.axis_c2c(X, B, Yh, Buf::kUserIn, Buf::kWs0) && b.rows_c2r(Y, B * X, Buf::kWs0, Buf::kUserOut);
+            break;
+        default:
+            b.err = "unsupported transform type";
+    }
+    return finish(p, b, ok);
+}
+
+std::string build_plan_3d(Plan &p)
+{
+    Builder b(p);
+    const int64_t B = p.batch, X = p.sizes[0], Y = p.sizes[1], Z = p.sizes[2];
+    const int64_t Zh = Z / 2 + 1;
+    bool ok = false;
+    switch (p.fft_type) {
+        case 0x10:
+            ok = b.axis_c2c(Z, B * X * Y, 1, Buf::kUserIn, Buf::kUserOut) &&
+                 b.axis_c2c(Y, B * X, Z, Buf::kUserOut, Buf::kUserOut) &&
+                 b.axis_c2c(X, B, Y * Z, Buf::kUserOut, Buf::kUserOut);
+            break;
+        case 0x12:
+            ok = b.rows_r2c(Z, B * X * Y, Buf::kUserIn, Buf::kUserOut) &&
+                 b.axis_c2c(Y, B * X, Zh, Buf::kUserOut, Buf::kUserOut) &&
+                 b.axis_c2c(X, B, Y * Zh, Buf::kUserOut, Buf::kUserOut);
+            break;
+        case 0x11:
+            b.need_ws(Buf::kWs0, size_t(B) * X * Y * Zh * sizeof(float2));
+            ok = b.axis_c2c(X, B, Y * Zh, Buf::kUserIn, Buf::kWs0) &&
+                 b.axis_c2c(Y, B * X, Zh, Buf::kWs0, Buf::kWs0) &&
+                 b.rows_c2r(Z, B * X * Y, Buf::kWs0, Buf::kUserOut);
+            break;
+        default:
+            b.err = "unsupported transform type";
+    }
+    return finish(p, b, ok);
+}
+
+std::string describe_plan(const Plan &p)
+{
+    std::ostringstream o;
+    o << "steps=" << p.steps.size() << " workspace=" << p.ws_bytes << "\n";
+    for (const Step &s : p.steps) {
+        o << "  [" << static_cast<int>(s.src) << "->" << static_cast<int>(s.dst) << "] " << s.what;
+        if (s.kind == StepKind::kTile) {
+            o << " n=" << s.d.n << " radices=";
+            for (int i = 0; i < s.d.nstages; i++) o << (i ? "x" : "") << s.d.radix[i];
+            o << " tb=" << s.d.tb << " tpt=" << s.d.tpt << " tiles=" << s.d.num_tiles << " grid=" << s.grid
+              << " smem=" << s.d.tb * s.d.pitch * 8;
+        }
+        o << "\n";
+    }
+    return o.str();
+}
+
+}  // namespace sipfft

@@ -1,0 +1,89 @@
+// Device-side runtime of the planner: the process-wide twiddle-table cache
+// and the step executor.
+//
+// Reference counterparts: FFTensorCache (core/fft/utils/fftensor_cache.cpp:20-92,
+// coefficient tensors shared across plans through weak pointers, built on the
+// host and copied to the device at plan time) and asdFftExecV2
+// (core/fft/fft_api.cpp:1001-1045, ping-pong of intermediate caches carved
+// from the caller's workspace).  Here the tables are generated directly on the
+// GPU in FP64 and rounded to FP32, and intermediate buffers are two fixed
+// slots of the caller's workspace.
+#include <map>
+#include <tuple>
+
+#include "sipfft_internal.h"
+
+namespace sipfft {
+
+DeviceTable::~DeviceTable()
+{
+    if (ptr) {
+        int cur = 0;
+        if (cudaGetDevice(&cur) == cudaSuccess && cur != device) cudaSetDevice(device);
+        cudaFree(ptr);
+        if (cur != device) cudaSetDevice(cur);
+        cudaGetLastError();  // a torn-down context at exit is not an error worth reporting
+    }
+}
+
+namespace {
+std::mutex g_table_mu;
+std::map<std::tuple<int, int64_t, int64_t, int64_t>, std::weak_ptr<DeviceTable>> g_tables;
+}  // namespace
+
+TablePtr get_table(int64_t count, int64_t denom, int64_t mult, int device, std::string *err)
+{
+    std::lock_guard<std::mutex> lock(g_table_mu);
+    auto key = std::make_tuple(device, count, denom, mult);
+    auto it = g_tables.find(key);
+    if (it != g_tables.end()) {
+        if (TablePtr t = it->second.lock()) return t;
+    }
+    auto t = std::make_shared<DeviceTable>();
+    t->count = count;
+    t->device = device;
+    cudaError_t e = cudaMalloc(&t->ptr, sizeof(float2) * static_cast<size_t>(count));
+    if (e == cudaSuccess) e = fill_twiddles(t->ptr, count, denom, mult, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) {
+        if (err) *err = std::string("twiddle table: ") + cudaGetErrorString(e);
+        cudaGetLastError();
+        return nullptr;
+    }
+    g_tables[key] = t;
+    return t;
+}
+
+cudaError_t execute_plan(Plan &p, const void *in, void *out, cudaStream_t st)
+{
+    char *ws = static_cast<char *>(p.workspace);
+    const size_t off1 = (p.ws_buf_bytes[0] + 255) / 256 * 256;
+    void *bufs[4] = {const_cast<void *>(in), out, ws, ws ? ws + off1 : nullptr};
+    for (const Step &s : p.steps) {
+        const void *src = bufs[static_cast<int>(s.src)];
+        void *dst = bufs[static_cast<int>(s.dst)];
+        if (src == nullptr || dst == nullptr) return cudaErrorInvalidDevicePointer;
+        cudaError_t e = cudaSuccess;
+        switch (s.kind) {
+            case StepKind::kTile: {
+                TileDesc d = s.d;
+                d.in = src;
+                d.out = dst;
+                e = launch_tile(d, s.maxe, s.forward, s.grid, st);
+                break;
+            }
+            case StepKind::kR2CPost:
+                e = launch_r2c_post(static_cast<const float2 *>(src), static_cast<float2 *>(dst), s.rows, s.m,
+                                    s.src_dist, s.dst_dist, s.lo, s.hi, s.log2l, s.forward, st);
+                break;
+            case StepKind::kC2RPre:
+                e = launch_c2r_pre(static_cast<const float2 *>(src), static_cast<float2 *>(dst), s.rows, s.m,
+                                   s.src_dist, s.dst_dist, s.lo, s.hi, s.log2l, s.forward, st);
+                break;
+        }
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace sipfft

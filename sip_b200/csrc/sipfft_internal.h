@@ -1,0 +1,95 @@
+// Internal declarations shared by the planner, the C-ABI layer and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "fft_tile.cuh"
+
+namespace sipfft {
+
+// Largest dynamic shared memory a CTA may use on sm_100 (227 KiB).
+constexpr int kMaxSmemBytes = 227 * 1024;
+// Number of SMs of a B200; the planner sizes persistent grids with the
+// queried count and falls back to this.
+constexpr int kB200Sms = 148;
+
+cudaError_t launch_tile(const TileDesc &d, int maxe, bool forward, int grid, cudaStream_t st);
+cudaError_t fill_twiddles(float2 *t, int64_t count, int64_t denom, int64_t mult, cudaStream_t st);
+// R2C post-twiddle / C2R pre-twiddle of the multi-pass (large-N) plans.
+cudaError_t launch_r2c_post(const float2 *z, float2 *x, int64_t rows, int64_t m, int64_t zdist, int64_t xdist,
+                            const float2 *tw_lo, const float2 *tw_hi, int log2l, bool forward, cudaStream_t st);
+cudaError_t launch_c2r_pre(const float2 *x, float2 *z, int64_t rows, int64_t m, int64_t xdist, int64_t zdist,
+                           const float2 *tw_lo, const float2 *tw_hi, int log2l, bool forward, cudaStream_t st);
+
+// A device twiddle table shared between plans (the reference's FFTensorCache,
+// core/fft/utils/fftensor_cache.cpp:55-92, keeps coefficient tensors alive
+// through weak pointers in the same way).
+struct DeviceTable {
+    float2 *ptr = nullptr;
+    int64_t count = 0;
+    int device = 0;
+    ~DeviceTable();
+};
+using TablePtr = std::shared_ptr<DeviceTable>;
+// t[m] = exp(-2 pi i (m*mult mod denom) / denom), m < count
+TablePtr get_table(int64_t count, int64_t denom, int64_t mult, int device, std::string *err);
+
+enum class Buf : int { kUserIn = 0, kUserOut = 1, kWs0 = 2, kWs1 = 3 };
+
+enum class StepKind : int { kTile = 0, kR2CPost = 1, kC2RPre = 2 };
+
+struct Step {
+    StepKind kind = StepKind::kTile;
+    TileDesc d{};
+    int maxe = 16;
+    int grid = 1;
+    bool forward = true;
+    Buf src = Buf::kUserIn;
+    Buf dst = Buf::kUserOut;
+    // kR2CPost / kC2RPre
+    int64_t rows = 0, m = 0, src_dist = 0, dst_dist = 0;
+    const float2 *lo = nullptr, *hi = nullptr;
+    int log2l = 0;
+    std::string what;  // human-readable description (plan dump)
+};
+
+struct Plan {
+    // reference FFTPlan fields (core/fft/fftplan/include/fftplan/fft_plan.h:49-70)
+    int fft_type = 0;
+    int direction = 0;
+    std::vector<int64_t> sizes;
+    std::vector<int64_t> strides;
+    int64_t batch = 0;
+    bool vertical = false;
+    void *stream = nullptr;
+    void *workspace = nullptr;
+    bool initialized = false;
+    bool failed = false;
+    // build-specific
+    int device = 0;
+    std::vector<Step> steps;
+    size_t ws_buf_bytes[2] = {0, 0};
+    size_t ws_bytes = 0;
+    std::vector<TablePtr> tables;
+    std::mutex mu;
+    bool forward() const;
+};
+
+// Planner entry points (planner.cpp).  They fill plan.steps / ws sizes and
+// return an empty string on success, else the reason.
+std::string build_plan_1d(Plan &p);
+std::string build_plan_2d(Plan &p);
+std::string build_plan_3d(Plan &p);
+// Launch every step of an initialised plan.
+cudaError_t execute_plan(Plan &p, const void *in, void *out, cudaStream_t st);
+std::string describe_plan(const Plan &p);
+
+// Radix decomposition used by the tile kernel (largest radices first).
+bool factor_radices(int64_t n, std::vector<int> &radices);
+
+}  // namespace sipfft

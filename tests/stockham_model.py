@@ -1,0 +1,133 @@
+"""NumPy model of the tile kernel's index arithmetic (test infrastructure).
+
+It replays, element by element, what sip_b200/csrc/fft_tile.cu does for one
+transform — the Stockham stage gather/scatter positions, the stage twiddle
+index r*(j mod Ns)*tstep, the multi-pass load/store addressing with the
+column-block jump, and the R2C/C2R pack twiddles — in complex128.  The CPU
+tests compare it with the oracle so that an indexing mistake is caught
+without a GPU.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def factor_radices(n: int) -> list[int]:
+    """Same decomposition as planner.cpp factor_radices()."""
+    m, twos = n, 0
+    while m % 2 == 0:
+        m //= 2
+        twos += 1
+    out = []
+    if twos:
+        s = (twos + 3) // 4
+        base, extra = divmod(twos, s)
+        out += [1 << (base + (1 if i < extra else 0)) for i in range(s)]
+    for p in (13, 11, 7, 5, 3):
+        while m % p == 0:
+            out.append(p)
+            m //= p
+    if m != 1:
+        raise ValueError(f"{n} has a prime factor above 13")
+    return out
+
+
+def table(denom: int, count: int, forward: bool, mult: int = 1) -> np.ndarray:
+    m = (np.arange(count, dtype=np.int64) * mult) % denom
+    w = np.exp(-2j * np.pi * m / denom)
+    return w if forward else np.conj(w)
+
+
+def dft_small(a: np.ndarray, forward: bool) -> np.ndarray:
+    r = a.shape[-1]
+    k = np.arange(r)
+    w = np.exp((-2j if forward else 2j) * np.pi * np.outer(k, k) / r)
+    return a @ w.T
+
+
+def smem_fft(row: np.ndarray, forward: bool, tw: np.ndarray, tw_mul: int) -> np.ndarray:
+    """Stockham stages exactly as stage_read/stage_write index them."""
+    n = row.shape[0]
+    x = row.astype(np.complex128).copy()
+    ns = 1
+    for r in factor_radices(n) if n > 1 else []:
+        nbf = n // r
+        tstep = (n // (ns * r)) * tw_mul
+        j = np.arange(nbf)
+        v = np.stack([x[j + q * nbf] for q in range(r)], axis=1)
+        if ns > 1:
+            step = (j % ns) * tstep
+            for q in range(1, r):
+                v[:, q] *= tw[q * step]
+        v = dft_small(v, forward)
+        k = j % ns
+        base = (j - k) * r + k
+        y = np.empty_like(x)
+        for q in range(r):
+            y[base + q * ns] = v[:, q]
+        x = y
+        ns *= r
+    return x
+
+
+def multipass(x: np.ndarray, passes: list[int], forward: bool) -> np.ndarray:
+    """Multi-pass Stockham over HBM: pass p reads columns j (stride F/Rp),
+    applies W_F^(r*(j mod Ns)*F/(Ns*Rp)), runs an Rp-point FFT and stores at
+    j + (j//Ns)*Ns*(Rp-1) + r*Ns."""
+    F = x.shape[0]
+    wF = table(F, F, forward)
+    cur = x.astype(np.complex128)
+    ns = 1
+    for rp in passes:
+        cols = F // rp
+        nxt = np.empty_like(cur)
+        twr = table(rp, rp, forward)
+        for c in range(cols):
+            e = np.arange(rp)
+            v = cur[c + e * cols]
+            if ns > 1:
+                v = v * wF[e * (c % ns) * (F // (ns * rp))]
+            v = smem_fft(v, forward, twr, 1)
+            nxt[c + (c // ns) * ns * (rp - 1) + e * ns] = v
+        cur = nxt
+        ns *= rp
+    return cur
+
+
+def r2c_packed(x: np.ndarray, forward: bool) -> np.ndarray:
+    n = x.shape[0]
+    m = n // 2
+    tw = table(n, n, forward)
+    z = smem_fft(x[0::2] + 1j * x[1::2], forward, tw, 2)
+    out = np.empty(m + 1, np.complex128)
+    for k in range(m // 2 + 1):
+        zk = z[k]
+        zm = np.conj(z[0 if k == 0 else m - k])
+        e = 0.5 * (zk + zm)
+        t = zk - zm
+        od = -0.5j * t
+        wo = tw[k] * od
+        out[k] = e + wo
+        if 2 * k != m:
+            out[m - k] = np.conj(e - wo)
+    return out
+
+
+def c2r_packed(xh: np.ndarray, n: int, forward: bool) -> np.ndarray:
+    m = n // 2
+    tw = table(n, n, forward)
+    z = np.empty(m, np.complex128)
+    for k in range(m // 2 + 1):
+        xk, xm = xh[k], xh[m - k]
+        if k == 0:
+            xk, xm = xk.real + 0j, xm.real + 0j
+        e = xk + np.conj(xm)
+        od = (xk - np.conj(xm)) * tw[k]
+        z[k] = e + 1j * od
+        if k != 0 and 2 * k != m:
+            z[m - k] = np.conj(e) + 1j * np.conj(od)
+    y = smem_fft(z, forward, tw, 2)
+    out = np.empty(n)
+    out[0::2] = y.real
+    out[1::2] = y.imag
+    return out

@@ -1,0 +1,229 @@
+"""GPU parity: the library's sm_100a kernels, called through the C ABI, against
+the FP64 oracle and against the reference's golden vectors.
+
+Bar: relative L2 error <= 1e-6 * log2(N) (N = product of the transform sizes),
+the accuracy gate the path is specified with; the golden vectors (FP32 outputs
+of the reference's FP32 matrices) get 2e-6 * log2(N).
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from sip_b200 import fft
+
+pytestmark = pytest.mark.gpu
+
+C2C, R2C, C2R = fft.ASCEND_FFT_C2C, fft.ASCEND_FFT_R2C, fft.ASCEND_FFT_C2R
+FWD, INV = fft.ASCEND_FFT_FORWARD, fft.ASCEND_FFT_INVERSE
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_vectors.npz")
+
+
+def _tol(sizes):
+    return oracle.tolerance(int(np.prod(sizes)))
+
+
+def _rand_complex(rng, shape):
+    return (rng.uniform(-1, 1, shape) + 1j * rng.uniform(-1, 1, shape)).astype(np.complex64)
+
+
+def run(sizes, typ, direction, batch, x, dim_type=fft.ASCEND_FFT_HORIZONTAL):
+    import torch
+
+    plan = fft.FftPlan(sizes, typ, direction, batch, dim_type)
+    try:
+        xin = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+        if typ == C2C:
+            out = torch.empty_like(xin)
+        elif typ == R2C:
+            out = torch.empty(x.shape[:-1] + (sizes[-1] // 2 + 1,), dtype=torch.complex64, device="cuda")
+        else:
+            out = torch.empty(x.shape[:-1] + (sizes[-1],), dtype=torch.float32, device="cuda")
+        plan(xin, out)
+        torch.cuda.synchronize()
+        return out.cpu().numpy()
+    finally:
+        plan.close()
+
+
+def check(sizes, typ, fwd, batch, seed=0, vertical=False):
+    rng = np.random.default_rng(seed)
+    nd = len(sizes)
+    f = fwd == FWD
+    if typ == C2C:
+        shape = (sizes[0], batch) if vertical else (batch, *sizes)
+        x = _rand_complex(rng, shape)
+        dim = fft.ASCEND_FFT_VERTICAL if vertical else fft.ASCEND_FFT_HORIZONTAL
+        y = run(sizes, typ, fwd, batch, x, dim)
+        ref = oracle.c2c(x.T, f).T if vertical else oracle.c2c(x, f, ndim=nd)
+    elif typ == R2C:
+        x = rng.standard_normal((batch, *sizes)).astype(np.float32)
+        y = run(sizes, typ, fwd, batch, x)
+        ref = oracle.r2c(x, f, ndim=nd)
+    else:
+        h = sizes[-1] // 2 + 1
+        x = (rng.standard_normal((batch, *sizes[:-1], h)) + 1j * rng.standard_normal((batch, *sizes[:-1], h)))
+        x = x.astype(np.complex64)
+        y = run(sizes, typ, fwd, batch, x)
+        ref = oracle.c2r(x, sizes[-1], f, ndim=nd)
+    err = oracle.rel_l2(y, ref)
+    assert err <= _tol(sizes), f"{sizes} type={typ:#x} dir={fwd:#x} batch={batch}: rel L2 {err:.3e}"
+    return err
+
+
+C2C_SIZES = [1, 2, 3, 4, 5, 7, 8, 11, 13, 16, 30, 64, 100, 128, 143, 210, 256, 343, 512, 1000, 1024, 1500,
+             2048, 3000, 4096, 6561, 8192, 10000, 15000, 16384, 24576, 32768, 65536, 3 * 2 ** 15, 2 ** 20]
+
+
+@pytest.mark.parametrize("n", C2C_SIZES)
+@pytest.mark.parametrize("fwd", [FWD, INV])
+def test_c2c_1d(cuda, n, fwd):
+    batch = 3 if n >= 4096 else 37
+    check([n], C2C, fwd, batch, seed=n)
+
+
+REAL_SIZES = [1, 2, 3, 4, 5, 6, 7, 30, 64, 100, 255, 256, 1000, 1024, 3000, 4096, 8192, 15625, 16384,
+              30000, 65536, 131072]
+
+
+@pytest.mark.parametrize("n", REAL_SIZES)
+@pytest.mark.parametrize("fwd", [FWD, INV])
+@pytest.mark.parametrize("typ", [R2C, C2R])
+def test_real_1d(cuda, n, fwd, typ):
+    batch = 3 if n >= 4096 else 21
+    check([n], typ, fwd, batch, seed=n + typ)
+
+
+@pytest.mark.parametrize("n,batch", [(256, 128), (1024, 200), (60, 33), (4096, 16)])
+@pytest.mark.parametrize("fwd", [FWD, INV])
+def test_c2c_vertical(cuda, n, batch, fwd):
+    check([n], C2C, fwd, batch, seed=n, vertical=True)
+
+
+SIZES_2D = [(1, 1), (3, 5), (32, 32), (64, 128), (100, 60), (2, 4096), (2048, 2048)]
+
+
+@pytest.mark.parametrize("xy", SIZES_2D)
+@pytest.mark.parametrize("typ", [C2C, R2C, C2R])
+@pytest.mark.parametrize("fwd", [FWD, INV])
+def test_2d(cuda, xy, typ, fwd):
+    batch = 1 if xy[0] * xy[1] > 100000 else 3
+    check(list(xy), typ, fwd, batch, seed=xy[0] * 7 + xy[1])
+
+
+SIZES_3D = [(2, 3, 4), (8, 16, 32), (16, 16, 16), (5, 7, 30), (256, 256, 256)]
+
+
+@pytest.mark.parametrize("xyz", SIZES_3D)
+@pytest.mark.parametrize("typ", [C2C, R2C, C2R])
+@pytest.mark.parametrize("fwd", [FWD, INV])
+def test_3d(cuda, xyz, typ, fwd):
+    batch = 1 if np.prod(xyz) > 100000 else 2
+    check(list(xyz), typ, fwd, batch, seed=int(np.prod(xyz)))
+
+
+def test_golden_vectors_through_library(cuda):
+    z = np.load(GOLDEN)
+    for name, kind, n, f in zip(z["_names"], z["_kinds"], z["_sizes"], z["_forward"]):
+        name, kind, n, f = str(name), str(kind), int(n), bool(f)
+        typ = {"c2c": C2C, "r2c": R2C, "c2r": C2R}[kind]
+        x = z[name + "__in"]
+        y = run([n], typ, FWD if f else INV, x.shape[0], x)
+        err = oracle.rel_l2(y, z[name + "__out"])
+        assert err <= 2e-6 * max(1.0, np.log2(max(n, 2))), (name, err)
+
+
+@pytest.mark.parametrize("n", [3000, 4096])
+def test_round_trip_full_size(cuda, n):
+    """C2R(INVERSE)(R2C(FORWARD)(x)) / N == x at the benchmark's full size (batch 4096)."""
+    import torch
+
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal((4096, n)).astype(np.float32)
+    f = fft.FftPlan([n], R2C, FWD, 4096)
+    g = fft.FftPlan([n], C2R, INV, 4096)
+    xd = torch.from_numpy(x).cuda()
+    X = torch.empty((4096, n // 2 + 1), dtype=torch.complex64, device="cuda")
+    y = torch.empty_like(xd)
+    f(xd, X)
+    g(X, y)
+    torch.cuda.synchronize()
+    err = oracle.rel_l2(y.cpu().numpy() / n, x)
+    assert err <= oracle.tolerance(n), err
+    # the forward half alone against the oracle on a subset of rows
+    ref = oracle.r2c(x[:64], True)
+    assert oracle.rel_l2(X[:64].cpu().numpy(), ref) <= oracle.tolerance(n)
+    f.close()
+    g.close()
+
+
+def test_in_place_c2c(cuda):
+    import torch
+
+    rng = np.random.default_rng(5)
+    for n, batch in [(1024, 64), (65536, 2)]:
+        x = _rand_complex(rng, (batch, n))
+        buf = torch.from_numpy(x).cuda()
+        plan = fft.FftPlan([n], C2C, FWD, batch)
+        assert plan.exec_raw(buf.data_ptr(), buf.data_ptr()) == fft.ACL_SUCCESS
+        torch.cuda.synchronize()
+        assert oracle.rel_l2(buf.cpu().numpy(), oracle.c2c(x, True)) <= oracle.tolerance(n)
+        plan.close()
+
+
+def test_many_rows_grid_loop(cuda):
+    """More tiles than the launch grid: the kernel's tile loop covers the rest."""
+    check([8], C2C, FWD, 300000, seed=11)
+    check([64], R2C, INV, 100000, seed=12)
+
+
+def test_exec_error_paths(cuda):
+    import torch
+
+    plan = fft.FftPlan([1024], C2C, FWD, 4)
+    x = torch.zeros((4, 1024), dtype=torch.complex64, device="cuda")
+    small = torch.zeros((3, 1024), dtype=torch.complex64, device="cuda")
+    wrong = torch.zeros((4, 512), dtype=torch.complex64, device="cuda")
+    real = torch.zeros((4, 1024), dtype=torch.float32, device="cuda")
+    for a, b in [(small, x), (x, small), (wrong, x), (real, x)]:
+        ta, tb = fft.AclTensor.from_torch(a), fft.AclTensor.from_torch(b)
+        assert fft.asdFftExecC2C(plan.handle, ta, tb) == fft.ACL_ERROR_INVALID_PARAM
+    # wrong exec kind for the plan type
+    ta, tb = fft.AclTensor.from_torch(real), fft.AclTensor.from_torch(x)
+    assert fft.asdFftExecR2C(plan.handle, ta, tb) == fft.ACL_ERROR_INVALID_PARAM
+    # misaligned device pointer
+    assert plan.exec_raw(x.data_ptr() + 4, x.data_ptr()) == fft.ACL_ERROR_INVALID_PARAM
+    plan.close()
+    # a plan that needs workspace refuses to run without it (fft_api.cpp:1008-1011)
+    h = fft.asdFftCreate()
+    assert fft.asdFftMakePlan1D(h, 65536, C2C, FWD, 1) == fft.ACL_SUCCESS
+    st, ws = fft.asdFftGetWorkspaceSize(h)
+    assert st == fft.ACL_SUCCESS and ws >= 65536 * 8
+    y = torch.zeros((1, 65536), dtype=torch.complex64, device="cuda")
+    assert fft.load_library().asdFftExecRaw(h, y.data_ptr(), y.data_ptr()) == fft.ACL_ERROR_INTERNAL_ERROR
+    assert fft.asdFftDestroy(h) == fft.ACL_SUCCESS
+    # unsupported length (prime factor 17) is refused at plan time, not at run time
+    h = fft.asdFftCreate()
+    assert fft.asdFftMakePlan1D(h, 17 * 19, C2C, FWD, 1) == fft.ACL_ERROR_API_NOT_SUPPORT
+    fft.asdFftDestroy(h)
+
+
+def test_stream_and_sync(cuda):
+    import torch
+
+    s = torch.cuda.Stream()
+    plan = fft.FftPlan([4096], C2C, INV, 8, stream=s)
+    rng = np.random.default_rng(3)
+    x = _rand_complex(rng, (8, 4096))
+    xd = torch.from_numpy(x).cuda()
+    y = torch.empty_like(xd)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        plan(xd, y)
+    assert fft.asdFftSynchronize(plan.handle) == fft.ACL_SUCCESS
+    assert oracle.rel_l2(y.cpu().numpy(), oracle.c2c(x, False)) <= oracle.tolerance(4096)
+    st, typ = fft.asdFftGetType(plan.handle)
+    assert st == fft.ACL_SUCCESS and typ == C2C
+    plan.close()

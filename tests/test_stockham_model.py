@@ -1,0 +1,38 @@
+"""CPU: the kernel's index arithmetic (replayed by tests/stockham_model.py)
+against the oracle, for the radix sets, multi-pass splits and R2C/C2R packing
+the planner emits."""
+import numpy as np
+import pytest
+
+import stockham_model as sm
+from oracle import oracle
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 7, 8, 11, 12, 13, 16, 30, 60, 64, 96, 100, 128, 143, 210,
+                               256, 343, 1000, 1024, 1500, 2048, 3000, 4096])
+@pytest.mark.parametrize("fwd", [True, False])
+def test_smem_stockham(n, fwd):
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    y = sm.smem_fft(x, fwd, sm.table(n, n, fwd), 1)
+    assert oracle.rel_l2(y, oracle.c2c(x, fwd)) < 1e-12
+
+
+@pytest.mark.parametrize("n,passes", [(64, [8, 8]), (96, [12, 8]), (1024, [32, 32]), (4096, [16, 16, 16]),
+                                      (3000, [60, 50]), (32768, [256, 128])])
+@pytest.mark.parametrize("fwd", [True, False])
+def test_multipass_addressing(n, passes, fwd):
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    y = sm.multipass(x, passes, fwd)
+    assert oracle.rel_l2(y, oracle.c2c(x, fwd)) < 1e-12
+
+
+@pytest.mark.parametrize("n", [2, 4, 6, 30, 64, 1000, 3000, 4096])
+@pytest.mark.parametrize("fwd", [True, False])
+def test_packed_real(n, fwd):
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal(n)
+    assert oracle.rel_l2(sm.r2c_packed(x, fwd), oracle.r2c(x, fwd)) < 1e-12
+    xh = rng.standard_normal(n // 2 + 1) + 1j * rng.standard_normal(n // 2 + 1)
+    assert oracle.rel_l2(sm.c2r_packed(xh, n, fwd), oracle.c2r(xh, n, fwd)) < 1e-12
