@@ -442,6 +442,16 @@ AspbStatus asdFftSynchronize(asdFftHandle handle)
         cudaGetLastError();
         return ACL_ERROR_INTERNAL_ERROR;
     }
+    // a bounded wait inside a kernel that gave up leaves a non-zero error word
+    if (int *w = sipfft::device_error_word(p->device)) {
+        int flag = 0;
+        if (cudaMemcpy(&flag, w, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && flag != 0) {
+            cudaMemset(w, 0, sizeof(int));
+            log_error("asdFftSynchronize", "a kernel wait timed out; results are incomplete");
+            return ACL_ERROR_INTERNAL_ERROR;
+        }
+        cudaGetLastError();
+    }
     return ACL_SUCCESS;
 }
 

@@ -197,8 +197,38 @@ struct Builder {
         d.tw = tw;
         d.tw_mul = tw_mul;
         s.grid = grid_for(d.num_tiles);
+        if (!column && n_outer == 1 && ia.estride == 1 && oa.estride == 1 &&
+            (io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
+            add_row_variant(s, c, ia.cstride, oa.cstride);
         p.steps.push_back(s);
         return true;
+    }
+
+    // TMA-pipelined persistent variant for contiguous rows: two staging
+    // buffers per CTA, each large enough for a tile in its HBM layout and in
+    // the padded work layout.
+    void add_row_variant(Step &s, const TileCfg &c, int64_t in_dist, int64_t out_dist)
+    {
+        const int64_t rows = s.d.n_cols;
+        for (int tb = c.tb; tb >= 1; tb /= 2) {
+            if ((tb * in_dist) % 2 != 0 && rows > tb) continue;  // full tiles must be 16-byte multiples
+            int64_t buf = std::max<int64_t>(tb * in_dist, int64_t(tb) * c.pitch);
+            buf = (buf + 1) / 2 * 2;
+            TileDesc d = s.d;
+            d.tb = tb;
+            d.num_tiles = (rows + tb - 1) / tb;
+            d.tiles_per_outer = d.num_tiles;
+            d.in_a = Addr{in_dist, 0, 1, 0, 0};
+            d.out_a = Addr{out_dist, 0, 1, 0, 0};
+            d.g_ns = buf;
+            if (row_kernel_smem(d) > static_cast<size_t>(kMaxSmemBytes)) continue;
+            const int per_sm = row_kernel_blocks_per_sm(d, s.maxe, s.forward);
+            if (per_sm <= 0) continue;
+            s.has_row = true;
+            s.rd = d;
+            s.row_grid = static_cast<int>(std::min<int64_t>(d.num_tiles, int64_t(per_sm) * sm_count(device)));
+            return;
+        }
     }
 
     Buf other_ws(Buf a, Buf b)
@@ -510,6 +540,8 @@ std::string describe_plan(const Plan &p)
             for (int i = 0; i < s.d.nstages; i++) o << (i ? "x" : "") << s.d.radix[i];
             o << " tb=" << s.d.tb << " tpt=" << s.d.tpt << " tiles=" << s.d.num_tiles << " grid=" << s.grid
               << " smem=" << s.d.tb * s.d.pitch * 8;
+            if (s.has_row)
+                o << " | row-pipelined tb=" << s.rd.tb << " grid=" << s.row_grid << " smem=" << row_kernel_smem(s.rd);
         }
         o << "\n";
     }

@@ -54,6 +54,41 @@ TablePtr get_table(int64_t count, int64_t denom, int64_t mult, int device, std::
     return t;
 }
 
+namespace {
+std::mutex g_dev_mu;
+std::map<int, int *> g_err_words;
+std::map<int, int> g_sms;
+}  // namespace
+
+int *device_error_word(int device)
+{
+    std::lock_guard<std::mutex> lock(g_dev_mu);
+    auto it = g_err_words.find(device);
+    if (it != g_err_words.end()) return it->second;
+    int *w = nullptr;
+    if (cudaMalloc(&w, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    cudaMemset(w, 0, sizeof(int));
+    g_err_words[device] = w;
+    return w;
+}
+
+int sm_count(int device)
+{
+    std::lock_guard<std::mutex> lock(g_dev_mu);
+    auto it = g_sms.find(device);
+    if (it != g_sms.end()) return it->second;
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        n = kB200Sms;
+    }
+    g_sms[device] = n;
+    return n;
+}
+
 cudaError_t execute_plan(Plan &p, const void *in, void *out, cudaStream_t st)
 {
     char *ws = static_cast<char *>(p.workspace);
@@ -66,10 +101,17 @@ cudaError_t execute_plan(Plan &p, const void *in, void *out, cudaStream_t st)
         cudaError_t e = cudaSuccess;
         switch (s.kind) {
             case StepKind::kTile: {
-                TileDesc d = s.d;
-                d.in = src;
-                d.out = dst;
-                e = launch_tile(d, s.maxe, s.forward, s.grid, st);
+                if (s.has_row && (reinterpret_cast<uintptr_t>(src) & 15) == 0 && src != dst) {
+                    TileDesc d = s.rd;
+                    d.in = src;
+                    d.out = dst;
+                    e = launch_row_tiles(d, s.maxe, s.forward, s.row_grid, device_error_word(p.device), st);
+                } else {
+                    TileDesc d = s.d;
+                    d.in = src;
+                    d.out = dst;
+                    e = launch_tile(d, s.maxe, s.forward, s.grid, st);
+                }
                 break;
             }
             case StepKind::kR2CPost:

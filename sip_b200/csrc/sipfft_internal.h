@@ -20,6 +20,16 @@ constexpr int kB200Sms = 148;
 
 cudaError_t launch_tile(const TileDesc &d, int maxe, bool forward, int grid, cudaStream_t st);
 cudaError_t fill_twiddles(float2 *t, int64_t count, int64_t denom, int64_t mult, cudaStream_t st);
+// TMA-pipelined persistent kernel for contiguous rows (row_fft.cu).  The row
+// descriptor keeps the row distance in in_a.dist / out_a.dist and the
+// per-buffer float2 count in g_ns.
+cudaError_t launch_row_tiles(const TileDesc &d, int maxe, bool forward, int grid, int *err, cudaStream_t st);
+size_t row_kernel_smem(const TileDesc &d);
+int row_kernel_blocks_per_sm(const TileDesc &d, int maxe, bool forward);
+// Process-wide device error word of the current device (bounded waits that
+// gave up set it); read and cleared by asdFftSynchronize.
+int *device_error_word(int device);
+int sm_count(int device);
 // R2C post-twiddle / C2R pre-twiddle of the multi-pass (large-N) plans.
 cudaError_t launch_r2c_post(const float2 *z, float2 *x, int64_t rows, int64_t m, int64_t zdist, int64_t xdist,
                             const float2 *tw_lo, const float2 *tw_hi, int log2l, bool forward, cudaStream_t st);
@@ -51,6 +61,11 @@ struct Step {
     bool forward = true;
     Buf src = Buf::kUserIn;
     Buf dst = Buf::kUserOut;
+    // optional TMA-pipelined row variant of the same step (used when the
+    // source pointer is 16-byte aligned)
+    bool has_row = false;
+    TileDesc rd{};
+    int row_grid = 1;
     // kR2CPost / kC2RPre
     int64_t rows = 0, m = 0, src_dist = 0, dst_dist = 0;
     const float2 *lo = nullptr, *hi = nullptr;
