@@ -11,27 +11,31 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Codelets are host-callable as well so that a CPU test can check every radix
+// against a direct DFT without a GPU.
+#define SIPFFT_HD __host__ __device__ __forceinline__
+
 namespace sipfft {
 
 // ---------------------------------------------------------------- complex helpers
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+SIPFFT_HD float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+SIPFFT_HD float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+SIPFFT_HD float2 cmul(float2 a, float2 b)
 {
     return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
-__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
-__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+SIPFFT_HD float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+SIPFFT_HD float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 // multiply by -i (FWD quarter turn) or +i
 template <bool FWD>
-__device__ __forceinline__ float2 mul_quarter(float2 a)
+SIPFFT_HD float2 mul_quarter(float2 a)
 {
     return FWD ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
 }
 // exp(sign * i * theta) with the direction's sign applied to a table entry
 // that holds exp(-i * theta).
 template <bool FWD>
-__device__ __forceinline__ float2 dir(float2 w)
+SIPFFT_HD float2 dir(float2 w)
 {
     return FWD ? w : make_float2(w.x, -w.y);
 }
@@ -75,7 +79,7 @@ struct Root {
 
 // multiply a by exp(-+ 2*pi*i*J/R) with the trivial angles special-cased
 template <int R, int J, bool FWD>
-__device__ __forceinline__ float2 rot(float2 a)
+SIPFFT_HD float2 rot(float2 a)
 {
     constexpr int j = ((J % R) + R) % R;
     if constexpr (j == 0) {
@@ -97,7 +101,7 @@ __device__ __forceinline__ float2 rot(float2 a)
 // Recursive radix-2 decimation in time on an array held in registers.
 template <int R, bool FWD>
 struct Pow2 {
-    __device__ __forceinline__ static void run(float2 *a)
+    SIPFFT_HD static void run(float2 *a)
     {
         float2 e[R / 2], o[R / 2];
 #pragma unroll
@@ -110,7 +114,7 @@ struct Pow2 {
         combine<0>(a, e, o);
     }
     template <int K>
-    __device__ __forceinline__ static void combine(float2 *a, const float2 *e, const float2 *o)
+    SIPFFT_HD static void combine(float2 *a, const float2 *e, const float2 *o)
     {
         if constexpr (K < R / 2) {
             float2 t = rot<R, K, FWD>(o[K]);
@@ -122,11 +126,11 @@ struct Pow2 {
 };
 template <bool FWD>
 struct Pow2<1, FWD> {
-    __device__ __forceinline__ static void run(float2 *) {}
+    SIPFFT_HD static void run(float2 *) {}
 };
 template <bool FWD>
 struct Pow2<2, FWD> {
-    __device__ __forceinline__ static void run(float2 *a)
+    SIPFFT_HD static void run(float2 *a)
     {
         float2 t = a[1];
         a[1] = csub(a[0], t);
@@ -135,7 +139,7 @@ struct Pow2<2, FWD> {
 };
 template <bool FWD>
 struct Pow2<4, FWD> {
-    __device__ __forceinline__ static void run(float2 *a)
+    SIPFFT_HD static void run(float2 *a)
     {
         float2 t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]);
         float2 t2 = cadd(a[1], a[3]), t3 = mul_quarter<FWD>(csub(a[1], a[3]));
@@ -154,7 +158,7 @@ struct Pow2<4, FWD> {
 template <int R, bool FWD>
 struct Odd {
     static constexpr int H = (R - 1) / 2;
-    __device__ __forceinline__ static void run(float2 *a)
+    SIPFFT_HD static void run(float2 *a)
     {
         float2 tp[H], tm[H];
 #pragma unroll
@@ -172,7 +176,7 @@ struct Odd {
         for (int i = 0; i < R; i++) a[i] = out[i];
     }
     template <int M>
-    __device__ __forceinline__ static void terms(float2 a0, const float2 *tp, const float2 *tm, float2 *out)
+    SIPFFT_HD static void terms(float2 a0, const float2 *tp, const float2 *tm, float2 *out)
     {
         if constexpr (M <= H) {
             float2 b = a0, d = make_float2(0.f, 0.f);
@@ -190,7 +194,7 @@ struct Odd {
         }
     }
     template <int M, int K>
-    __device__ __forceinline__ static void accum(float2 &b, float2 &d, const float2 *tp, const float2 *tm)
+    SIPFFT_HD static void accum(float2 &b, float2 &d, const float2 *tp, const float2 *tm)
     {
         if constexpr (K <= H) {
             constexpr float c = Root<R, (K * M) % R>::c;
@@ -206,7 +210,7 @@ struct Odd {
 
 template <bool FWD>
 struct Odd<3, FWD> {
-    __device__ __forceinline__ static void run(float2 *a)
+    SIPFFT_HD static void run(float2 *a)
     {
         constexpr float h = 0.86602540378443864676f;  // sqrt(3)/2
         float2 s = cadd(a[1], a[2]);
@@ -230,13 +234,75 @@ struct Odd<3, FWD> {
 template <int R>
 constexpr bool is_pow2() { return R > 0 && (R & (R - 1)) == 0; }
 
+constexpr int smallest_prime_factor(int r)
+{
+    for (int p = 2; p * p <= r; p++)
+        if (r % p == 0) return p;
+    return r;
+}
+// split of a composite radix R = A * B used by Comp: the power-of-two part
+// first for even R, else the smallest prime factor
+constexpr int comp_first(int r)
+{
+    if (r % 2 == 0) {
+        int a = 1;
+        while (r % (2 * a) == 0) a *= 2;
+        return a;
+    }
+    return smallest_prime_factor(r);
+}
+
 template <int R, bool FWD>
-__device__ __forceinline__ void dft(float2 *a)
+SIPFFT_HD void dft(float2 *a);
+
+// Composite radix R = A*B in registers (Cooley-Tukey, decimation in time):
+// B-point DFTs over the A interleaved sub-sequences, twiddles W_R^(n1*k2),
+// then A-point DFTs; output index k = k2 + B*k1.
+template <int A, int B, bool FWD>
+struct Comp {
+    static constexpr int R = A * B;
+    SIPFFT_HD static void run(float2 *a)
+    {
+        float2 y[A][B];
+#pragma unroll
+        for (int n1 = 0; n1 < A; n1++) {
+#pragma unroll
+            for (int n2 = 0; n2 < B; n2++) y[n1][n2] = a[n1 + A * n2];
+            dft<B, FWD>(y[n1]);
+        }
+        twiddle<1, 1>(y);
+#pragma unroll
+        for (int k2 = 0; k2 < B; k2++) {
+            float2 z[A];
+#pragma unroll
+            for (int n1 = 0; n1 < A; n1++) z[n1] = y[n1][k2];
+            dft<A, FWD>(z);
+#pragma unroll
+            for (int k1 = 0; k1 < A; k1++) a[k2 + B * k1] = z[k1];
+        }
+    }
+    template <int N1, int K2>
+    SIPFFT_HD static void twiddle(float2 (&y)[A][B])
+    {
+        if constexpr (N1 < A) {
+            if constexpr (K2 < B) {
+                y[N1][K2] = rot<R, N1 * K2, FWD>(y[N1][K2]);
+                twiddle<N1, K2 + 1>(y);
+            } else {
+                twiddle<N1 + 1, 1>(y);
+            }
+        }
+    }
+};
+
+template <int R, bool FWD>
+SIPFFT_HD void dft(float2 *a)
 {
     if constexpr (is_pow2<R>()) {
         Pow2<R, FWD>::run(a);
+    } else if constexpr (R % 2 == 0 || (smallest_prime_factor(R) != R && R > 13)) {
+        Comp<comp_first(R), R / comp_first(R), FWD>::run(a);
     } else {
-        static_assert(R % 2 == 1, "composite even radices are split into stages by the planner");
         Odd<R, FWD>::run(a);
     }
 }

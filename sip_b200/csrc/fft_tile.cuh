@@ -68,6 +68,10 @@ struct TileDesc {
     int64_t g_step;    // F / (g_ns * n)
     const float2 *g_lo;
     const float2 *g_hi;
+    // Per-stage twiddle tables of the compile-time (static) kernels: stage s
+    // occupies (R_s - 1) * Ns_s entries laid out [r-1][k], value
+    // exp(-2 pi i r k / (Ns_s R_s)), so a warp's loads for one r are contiguous.
+    const float2 *stw;
 };
 
 }  // namespace sipfft

@@ -1,0 +1,157 @@
+// Persistent, TMA-pipelined FFT kernel skeleton for batched contiguous rows
+// (the 1D hot path: C2C, and even-length R2C / C2R through the packed
+// n/2-point FFT).
+//
+// Each CTA walks its tiles (tb consecutive rows) with two shared-memory
+// buffers: while tile i is transformed in buffer i&1, the bulk-copy engine
+// (cp.async.bulk, completion on an mbarrier) streams tile i+grid into the
+// other buffer, so HBM reads run continuously under the butterflies.  Stage 0
+// reads the staged rows in their HBM layout (C2R: pre-twiddled pairs computed
+// on the fly), the remaining stages run in the padded work layout of the same
+// buffer, and the last stage writes HBM directly (C2C, C2R) or, for R2C, the
+// post-twiddle pass writes the N/2+1 bins.  One HBM read and one HBM write per
+// element.
+//
+// The butterfly engine is a template parameter: RuntimeEngine (radices read
+// from the descriptor) or a compile-time StaticEngine (static_fft.cu).
+#pragma once
+#include "async_copy.cuh"
+#include "sipfft_internal.h"
+#include "stages.cuh"
+
+namespace sipfft {
+
+// staged row in its HBM layout (unpadded)
+struct StageRow {
+    const float2 *row;
+    __device__ __forceinline__ float2 operator()(int e) const { return row[e]; }
+};
+
+// C2R input seen as the packed m-point sequence Z (computed from X[e], X[m-e])
+template <bool FWD>
+struct C2RPre {
+    const float2 *x;  // staged half spectrum, m+1 bins
+    int m;
+    const float2 *tw;  // exp(-2 pi i k / 2m)
+    __device__ __forceinline__ float2 operator()(int e) const
+    {
+        float2 xk = x[e];
+        float2 xm = x[m - e];
+        if (e == 0) {
+            xk.y = 0.f;
+            xm.y = 0.f;
+        }
+        const float2 ev = cadd(xk, cconj(xm));
+        const float2 od = cmul(csub(xk, cconj(xm)), dir<FWD>(__ldg(tw + e)));
+        return make_float2(ev.x - od.y, ev.y + od.x);
+    }
+};
+
+struct GlobalRow {
+    float2 *row;
+    __device__ __forceinline__ void operator()(int e, float2 v) const { row[e] = v; }
+};
+
+template <int MAXE>
+struct RuntimeEngine {
+    template <bool FWD, class Src0, class DstL>
+    __device__ __forceinline__ static void run(const TileDesc &d, float2 *work, const Src0 &src0, const DstL &dstL,
+                                               bool dst_in_place, int lane, bool active)
+    {
+        run_fft<MAXE, FWD>(d, work, src0, true, dstL, dst_in_place, lane, active);
+    }
+};
+
+// R2C post-twiddle from the padded work row to HBM: X[k] = E + w^k O,
+// X[n-k] = conj(E - w^k O) with E, O recovered from Z[k], conj(Z[n-k]).
+template <bool FWD>
+__device__ __forceinline__ void r2c_post_row(const float2 *work, float2 *y, int n, int lane, int tpt,
+                                             const float2 *tw)
+{
+    for (int k = lane; 2 * k <= n; k += tpt) {
+        const float2 zk = work[pad(k)];
+        const float2 zm = cconj(work[pad(k == 0 ? 0 : n - k)]);
+        const float2 e = cscale(cadd(zk, zm), 0.5f);
+        const float2 tt = csub(zk, zm);
+        const float2 od = make_float2(0.5f * tt.y, -0.5f * tt.x);
+        const float2 wo = cmul(dir<FWD>(__ldg(tw + k)), od);
+        y[k] = cadd(e, wo);
+        if (2 * k != n) y[n - k] = cconj(csub(e, wo));
+    }
+}
+
+template <class Engine, bool FWD, int IO>
+__global__ void __launch_bounds__(512, 1) pipelined_rows_kernel(const __grid_constant__ TileDesc d, int *err)
+{
+    extern __shared__ __align__(128) unsigned char smraw[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smraw);
+    const int64_t buf_f2 = d.g_ns;  // per-buffer float2 count (planner-computed, even)
+    float2 *bufs = reinterpret_cast<float2 *>(smraw + 128);
+    const int tid = threadIdx.x;
+    const int tb = d.tb, tpt = d.tpt;
+    const int l = tid / tpt, lane = tid % tpt;
+    const bool thread_on = tid < tb * tpt;
+    const int64_t in_dist = d.in_a.dist, out_dist = d.out_a.dist;
+    const int64_t rows_total = d.n_cols;
+    const float2 *in = static_cast<const float2 *>(d.in);
+    float2 *out = static_cast<float2 *>(d.out);
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    // Bytes of tile t that the bulk engine copies (a multiple of 16); a
+    // trailing 8-byte element, if any, is fetched with a plain load.
+    auto tile_rows = [&](int64_t t) -> int {
+        const int64_t left = rows_total - t * tb;
+        return left < tb ? static_cast<int>(left) : tb;
+    };
+    auto issue = [&](int64_t t, int b) {
+        if (tid == 0) {
+            const uint32_t bytes = static_cast<uint32_t>(tile_rows(t) * in_dist * 8);
+            const uint32_t bulk = bytes & ~15u;
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&bars[b], bulk);
+            if (bulk) bulk_g2s(bufs + b * buf_f2, in + t * tb * in_dist, bulk, &bars[b]);
+        }
+    };
+
+    int64_t t = blockIdx.x;
+    if (t < d.num_tiles) issue(t, 0);
+    for (int i = 0; t < d.num_tiles; t += gridDim.x, i++) {
+        const int b = i & 1;
+        const int64_t tn = t + gridDim.x;
+        if (tn < d.num_tiles) issue(tn, b ^ 1);
+        if (!mbar_wait_bounded(&bars[b], (i >> 1) & 1)) {
+            if (tid == 0) atomicExch(err, 1);
+            return;
+        }
+        const int rows = tile_rows(t);
+        float2 *buf = bufs + b * buf_f2;
+        const int64_t bytes = rows * in_dist * 8;
+        if (bytes & 15) {  // uniform across the CTA
+            if (tid == 0) buf[rows * in_dist - 1] = in[t * tb * in_dist + rows * in_dist - 1];
+            __syncthreads();
+        }
+        const bool active = thread_on && l < rows;
+        float2 *work = buf + l * d.pitch;
+        const int64_t row_index = t * tb + l;
+        if constexpr (IO == IO_C2C) {
+            Engine::template run<FWD>(d, work, StageRow{buf + l * in_dist}, GlobalRow{out + row_index * out_dist},
+                                      false, lane, active);
+        } else if constexpr (IO == IO_C2R_PACKED) {
+            Engine::template run<FWD>(d, work, C2RPre<FWD>{buf + l * in_dist, d.n, d.tw},
+                                      GlobalRow{out + row_index * out_dist}, false, lane, active);
+        } else {  // IO_R2C_PACKED: FFT into the work rows, then the post-twiddle to HBM
+            Engine::template run<FWD>(d, work, StageRow{buf + l * in_dist}, SmemRow{work}, true, lane, active);
+            __syncthreads();
+            if (active) r2c_post_row<FWD>(work, out + row_index * out_dist, d.n, lane, tpt, d.tw);
+        }
+        __syncthreads();  // buffer b is free for the copy issued in iteration i+1
+    }
+}
+
+}  // namespace sipfft

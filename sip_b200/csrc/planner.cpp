@@ -207,9 +207,25 @@ struct Builder {
     // TMA-pipelined persistent variant for contiguous rows: two staging
     // buffers per CTA, each large enough for a tile in its HBM layout and in
     // the padded work layout.
-    void add_row_variant(Step &s, const TileCfg &c, int64_t in_dist, int64_t out_dist)
+    void add_row_variant(Step &s, const TileCfg &c0, int64_t in_dist, int64_t out_dist)
     {
         const int64_t rows = s.d.n_cols;
+        TileCfg c = c0;
+        const StaticKernel *sk = find_static_kernel(s.d.n);
+        const float2 *stw = nullptr;
+        if (sk) {
+            TablePtr t = get_stage_table(*sk, device, &err);
+            if (t) {
+                p.tables.push_back(t);
+                stw = t->ptr;
+                c.tpt = sk->tpt;
+                c.tb = std::max(1, std::min(kRowThreadsTarget / sk->tpt, static_cast<int>(std::min<int64_t>(rows, 64))));
+                while (c.tb > 1 && c.tb * c.tpt > kMaxThreads) c.tb /= 2;
+            } else {
+                sk = nullptr;
+                err.clear();
+            }
+        }
         for (int tb = c.tb; tb >= 1; tb /= 2) {
             if ((tb * in_dist) % 2 != 0 && rows > tb) continue;  // full tiles must be 16-byte multiples
             int64_t buf = std::max<int64_t>(tb * in_dist, int64_t(tb) * c.pitch);
@@ -221,10 +237,19 @@ struct Builder {
             d.in_a = Addr{in_dist, 0, 1, 0, 0};
             d.out_a = Addr{out_dist, 0, 1, 0, 0};
             d.g_ns = buf;
+            d.tpt = c.tpt;
             if (row_kernel_smem(d) > static_cast<size_t>(kMaxSmemBytes)) continue;
-            const int per_sm = row_kernel_blocks_per_sm(d, s.maxe, s.forward);
+            const void *fn = nullptr;
+            if (sk) {
+                const int io = d.io == IO_C2C ? 0 : (d.io == IO_R2C_PACKED ? 1 : 2);
+                fn = sk->fn[s.forward ? 1 : 0][io];
+                d.stw = stw;
+            }
+            const int per_sm = fn ? kernel_blocks_per_sm(fn, tb * c.tpt, row_kernel_smem(d))
+                                  : row_kernel_blocks_per_sm(d, s.maxe, s.forward);
             if (per_sm <= 0) continue;
             s.has_row = true;
+            s.row_fn = fn;
             s.rd = d;
             s.row_grid = static_cast<int>(std::min<int64_t>(d.num_tiles, int64_t(per_sm) * sm_count(device)));
             return;
@@ -541,7 +566,8 @@ std::string describe_plan(const Plan &p)
             o << " tb=" << s.d.tb << " tpt=" << s.d.tpt << " tiles=" << s.d.num_tiles << " grid=" << s.grid
               << " smem=" << s.d.tb * s.d.pitch * 8;
             if (s.has_row)
-                o << " | row-pipelined tb=" << s.rd.tb << " grid=" << s.row_grid << " smem=" << row_kernel_smem(s.rd);
+                o << " | row-pipelined" << (s.row_fn ? " static" : "") << " tb=" << s.rd.tb << " tpt=" << s.rd.tpt
+                  << " grid=" << s.row_grid << " smem=" << row_kernel_smem(s.rd);
         }
         o << "\n";
     }

@@ -1,210 +1,77 @@
-// Persistent, TMA-pipelined FFT kernel for batched contiguous rows (the 1D
-// hot path: C2C, and even-length R2C / C2R through the packed n/2-point FFT).
-//
-// Each CTA walks its tiles (tb consecutive rows) with two shared-memory
-// buffers: while tile i is transformed in buffer i&1, the bulk-copy engine
-// (cp.async.bulk, completion on an mbarrier) streams tile i+grid into the
-// other buffer, so HBM reads run continuously under the butterflies.  Stage 0
-// reads the staged rows in their HBM layout (C2R: pre-twiddled pairs computed
-// on the fly), the remaining stages run in the padded work layout of the same
-// buffer, and the last stage writes HBM directly (C2C, C2R) or, for R2C,
-// the post-twiddle pass writes the N/2+1 bins.  One HBM read and one HBM
-// write per element.
-#include "async_copy.cuh"
-#include "sipfft_internal.h"
-#include "stages.cuh"
+// Runtime-radix instantiation of the TMA-pipelined row kernel
+// (pipelined_rows.cuh) and its host-side launch helpers.
+#include "pipelined_rows.cuh"
 
 namespace sipfft {
 
 namespace {
 
-// staged row in its HBM layout (unpadded)
-struct StageRow {
-    const float2 *row;
-    __device__ __forceinline__ float2 operator()(int e) const { return row[e]; }
-};
-
-// C2R input seen as the packed m-point sequence Z (computed from X[e], X[m-e])
-template <bool FWD>
-struct C2RPre {
-    const float2 *x;  // staged half spectrum, m+1 bins
-    int m;
-    const float2 *tw;  // exp(-2 pi i k / 2m)
-    __device__ __forceinline__ float2 operator()(int e) const
-    {
-        float2 xk = x[e];
-        float2 xm = x[m - e];
-        if (e == 0) {
-            xk.y = 0.f;
-            xm.y = 0.f;
-        }
-        const float2 ev = cadd(xk, cconj(xm));
-        const float2 od = cmul(csub(xk, cconj(xm)), dir<FWD>(__ldg(tw + e)));
-        return make_float2(ev.x - od.y, ev.y + od.x);
-    }
-};
-
-struct GlobalRow {
-    float2 *row;
-    __device__ __forceinline__ void operator()(int e, float2 v) const { row[e] = v; }
-};
-
-}  // namespace
-
 template <int MAXE, bool FWD, int IO>
-__global__ void __launch_bounds__(512, 1) row_fft_kernel(const __grid_constant__ TileDesc d, int *err)
+const void *row_fn()
 {
-    extern __shared__ __align__(128) unsigned char smraw[];
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smraw);
-    const int64_t buf_f2 = d.g_ns;  // per-buffer float2 count (planner-computed, even)
-    float2 *bufs = reinterpret_cast<float2 *>(smraw + 128);
-    const int tid = threadIdx.x;
-    const int tb = d.tb, tpt = d.tpt;
-    const int l = tid / tpt, lane = tid % tpt;
-    const bool thread_on = tid < tb * tpt;
-    const int64_t in_dist = d.in_a.dist, out_dist = d.out_a.dist;
-    const int64_t rows_total = d.n_cols;
-    const float2 *in = static_cast<const float2 *>(d.in);
-    float2 *out = static_cast<float2 *>(d.out);
-
-    if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
-
-    // bytes of tile t that the bulk engine copies (a multiple of 16); a
-    // trailing 8-byte element, if any, is fetched with a plain load.
-    auto tile_rows = [&](int64_t t) -> int {
-        const int64_t left = rows_total - t * tb;
-        return left < tb ? static_cast<int>(left) : tb;
-    };
-    auto issue = [&](int64_t t, int b) {
-        if (tid == 0) {
-            const uint32_t bytes = static_cast<uint32_t>(tile_rows(t) * in_dist * 8);
-            const uint32_t bulk = bytes & ~15u;
-            fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&bars[b], bulk);
-            if (bulk) bulk_g2s(bufs + b * buf_f2, in + t * tb * in_dist, bulk, &bars[b]);
-        }
-    };
-
-    int64_t t = blockIdx.x;
-    if (t < d.num_tiles) issue(t, 0);
-    for (int i = 0; t < d.num_tiles; t += gridDim.x, i++) {
-        const int b = i & 1;
-        const int64_t tn = t + gridDim.x;
-        if (tn < d.num_tiles) issue(tn, b ^ 1);
-        if (!mbar_wait_bounded(&bars[b], (i >> 1) & 1)) {
-            if (tid == 0) atomicExch(err, 1);
-            return;
-        }
-        const int rows = tile_rows(t);
-        float2 *buf = bufs + b * buf_f2;
-        const int64_t bytes = rows * in_dist * 8;
-        if (bytes & 15) {  // uniform across the CTA
-            if (tid == 0) buf[rows * in_dist - 1] = in[t * tb * in_dist + rows * in_dist - 1];
-            __syncthreads();
-        }
-        const bool active = thread_on && l < rows;
-        float2 *work = buf + l * d.pitch;
-        const int64_t row_index = t * tb + l;
-        if constexpr (IO == IO_C2C) {
-            run_fft<MAXE, FWD>(d, work, StageRow{buf + l * in_dist}, true, GlobalRow{out + row_index * out_dist},
-                               false, lane, active);
-        } else if constexpr (IO == IO_C2R_PACKED) {
-            run_fft<MAXE, FWD>(d, work, C2RPre<FWD>{buf + l * in_dist, d.n, d.tw}, true,
-                               GlobalRow{out + row_index * out_dist}, false, lane, active);
-        } else {  // IO_R2C_PACKED: FFT into the work rows, then the post-twiddle to HBM
-            run_fft<MAXE, FWD>(d, work, StageRow{buf + l * in_dist}, true, SmemRow{work}, true, lane, active);
-            __syncthreads();
-            if (active) {
-                const int n = d.n;
-                float2 *y = out + row_index * out_dist;
-                for (int k = lane; 2 * k <= n; k += tpt) {
-                    const float2 zk = work[pad(k)];
-                    const float2 zm = cconj(work[pad(k == 0 ? 0 : n - k)]);
-                    const float2 e = cscale(cadd(zk, zm), 0.5f);
-                    const float2 tt = csub(zk, zm);
-                    const float2 od = make_float2(0.5f * tt.y, -0.5f * tt.x);
-                    const float2 wo = cmul(dir<FWD>(__ldg(d.tw + k)), od);
-                    y[k] = cadd(e, wo);
-                    if (2 * k != n) y[n - k] = cconj(csub(e, wo));
-                }
-            }
-        }
-        __syncthreads();  // buffer b is free for the copy issued in iteration i+1
-    }
-}
-
-namespace {
-template <int MAXE, bool FWD, int IO>
-cudaError_t launch_row(const TileDesc &d, int grid, size_t smem, int *err, cudaStream_t st)
-{
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(row_fft_kernel<MAXE, FWD, IO>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBytes);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
-    row_fft_kernel<MAXE, FWD, IO><<<grid, d.tb * d.tpt, smem, st>>>(d, err);
-    return cudaGetLastError();
+    return reinterpret_cast<const void *>(pipelined_rows_kernel<RuntimeEngine<MAXE>, FWD, IO>);
 }
 
 template <int MAXE, bool FWD>
-cudaError_t launch_row_io(const TileDesc &d, int grid, size_t smem, int *err, cudaStream_t st)
+const void *row_fn_io(int io)
 {
-    switch (d.io) {
-        case IO_C2C: return launch_row<MAXE, FWD, IO_C2C>(d, grid, smem, err, st);
-        case IO_R2C_PACKED: return launch_row<MAXE, FWD, IO_R2C_PACKED>(d, grid, smem, err, st);
-        case IO_C2R_PACKED: return launch_row<MAXE, FWD, IO_C2R_PACKED>(d, grid, smem, err, st);
-        default: return cudaErrorInvalidValue;
+    switch (io) {
+        case IO_C2C: return row_fn<MAXE, FWD, IO_C2C>();
+        case IO_R2C_PACKED: return row_fn<MAXE, FWD, IO_R2C_PACKED>();
+        case IO_C2R_PACKED: return row_fn<MAXE, FWD, IO_C2R_PACKED>();
+        default: return nullptr;
     }
 }
+
+const void *pick(const TileDesc &d, int maxe, bool forward)
+{
+    if (maxe <= 8) return forward ? row_fn_io<8, true>(d.io) : row_fn_io<8, false>(d.io);
+    if (maxe <= 16) return forward ? row_fn_io<16, true>(d.io) : row_fn_io<16, false>(d.io);
+    return forward ? row_fn_io<32, true>(d.io) : row_fn_io<32, false>(d.io);
+}
+
 }  // namespace
 
 size_t row_kernel_smem(const TileDesc &d) { return 128 + 2 * static_cast<size_t>(d.g_ns) * sizeof(float2); }
 
-int row_kernel_blocks_per_sm(const TileDesc &d, int maxe, bool forward)
+int kernel_blocks_per_sm(const void *fn, int threads, size_t smem)
 {
     int nb = 0;
-    const size_t smem = row_kernel_smem(d);
-    const int threads = d.tb * d.tpt;
-    const void *fn = nullptr;
-#define SIPFFT_PICK(M)                                                                              \
-    if (maxe <= M) {                                                                                \
-        if (d.io == IO_C2C) fn = forward ? (const void *)row_fft_kernel<M, true, IO_C2C>            \
-                                         : (const void *)row_fft_kernel<M, false, IO_C2C>;          \
-        else if (d.io == IO_R2C_PACKED) fn = forward ? (const void *)row_fft_kernel<M, true, IO_R2C_PACKED> \
-                                                     : (const void *)row_fft_kernel<M, false, IO_R2C_PACKED>; \
-        else fn = forward ? (const void *)row_fft_kernel<M, true, IO_C2R_PACKED>                    \
-                          : (const void *)row_fft_kernel<M, false, IO_C2R_PACKED>;                  \
-    }
-    SIPFFT_PICK(32)
-    SIPFFT_PICK(16)
-    SIPFFT_PICK(8)
-#undef SIPFFT_PICK
     if (!fn) return 0;
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBytes);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBytes) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     return nb;
 }
 
+cudaError_t launch_kernel_fn(const void *fn, const TileDesc &d, int grid, size_t smem, int *err, cudaStream_t st)
+{
+    if (!fn || d.tb * d.tpt > 512 || smem > static_cast<size_t>(kMaxSmemBytes) || grid <= 0)
+        return cudaErrorInvalidConfiguration;
+    TileDesc dd = d;
+    void *args[] = {&dd, &err};
+    return cudaLaunchKernel(fn, dim3(grid), dim3(d.tb * d.tpt), args, smem, st);
+}
+
+int row_kernel_blocks_per_sm(const TileDesc &d, int maxe, bool forward)
+{
+    return kernel_blocks_per_sm(pick(d, maxe, forward), d.tb * d.tpt, row_kernel_smem(d));
+}
+
 cudaError_t launch_row_tiles(const TileDesc &d, int maxe, bool forward, int grid, int *err, cudaStream_t st)
 {
-    const size_t smem = row_kernel_smem(d);
-    if (d.tb * d.tpt > 512 || smem > static_cast<size_t>(kMaxSmemBytes) || grid <= 0)
-        return cudaErrorInvalidConfiguration;
-    if (maxe <= 8) return forward ? launch_row_io<8, true>(d, grid, smem, err, st)
-                                  : launch_row_io<8, false>(d, grid, smem, err, st);
-    if (maxe <= 16) return forward ? launch_row_io<16, true>(d, grid, smem, err, st)
-                                   : launch_row_io<16, false>(d, grid, smem, err, st);
-    return forward ? launch_row_io<32, true>(d, grid, smem, err, st) : launch_row_io<32, false>(d, grid, smem, err, st);
+    const void *fn = pick(d, maxe, forward);
+    static bool configured[3][2][3] = {};
+    const int mi = maxe <= 8 ? 0 : (maxe <= 16 ? 1 : 2);
+    const int ii = d.io == IO_C2C ? 0 : (d.io == IO_R2C_PACKED ? 1 : 2);
+    if (!configured[mi][forward][ii]) {
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBytes) != cudaSuccess)
+            return cudaGetLastError();
+        configured[mi][forward][ii] = true;
+    }
+    return launch_kernel_fn(fn, d, grid, row_kernel_smem(d), err, st);
 }
 
 }  // namespace sipfft

@@ -54,6 +54,31 @@ TablePtr get_table(int64_t count, int64_t denom, int64_t mult, int device, std::
     return t;
 }
 
+TablePtr get_stage_table(const StaticKernel &k, int device, std::string *err)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, std::weak_ptr<DeviceTable>> cache;  // (device, n)
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_pair(device, k.n);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+        if (TablePtr t = it->second.lock()) return t;
+    }
+    auto t = std::make_shared<DeviceTable>();
+    t->count = std::max<int64_t>(1, stage_twiddle_count(k.radix, k.nstages));
+    t->device = device;
+    cudaError_t e = cudaMalloc(&t->ptr, sizeof(float2) * static_cast<size_t>(t->count));
+    if (e == cudaSuccess) e = fill_stage_twiddles(t->ptr, k.radix, k.nstages, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) {
+        if (err) *err = std::string("twiddle table: ") + cudaGetErrorString(e);
+        cudaGetLastError();
+        return nullptr;
+    }
+    cache[key] = t;
+    return t;
+}
+
 namespace {
 std::mutex g_dev_mu;
 std::map<int, int *> g_err_words;
@@ -105,7 +130,11 @@ cudaError_t execute_plan(Plan &p, const void *in, void *out, cudaStream_t st)
                     TileDesc d = s.rd;
                     d.in = src;
                     d.out = dst;
-                    e = launch_row_tiles(d, s.maxe, s.forward, s.row_grid, device_error_word(p.device), st);
+                    if (s.row_fn)
+                        e = launch_kernel_fn(s.row_fn, d, s.row_grid, row_kernel_smem(d), device_error_word(p.device),
+                                             st);
+                    else
+                        e = launch_row_tiles(d, s.maxe, s.forward, s.row_grid, device_error_word(p.device), st);
                 } else {
                     TileDesc d = s.d;
                     d.in = src;

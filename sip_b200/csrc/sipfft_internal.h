@@ -26,6 +26,20 @@ cudaError_t fill_twiddles(float2 *t, int64_t count, int64_t denom, int64_t mult,
 cudaError_t launch_row_tiles(const TileDesc &d, int maxe, bool forward, int grid, int *err, cudaStream_t st);
 size_t row_kernel_smem(const TileDesc &d);
 int row_kernel_blocks_per_sm(const TileDesc &d, int maxe, bool forward);
+int kernel_blocks_per_sm(const void *fn, int threads, size_t smem);
+cudaError_t launch_kernel_fn(const void *fn, const TileDesc &d, int grid, size_t smem, int *err, cudaStream_t st);
+
+// Compile-time specialised pipelined row kernels (static_fft.cu).
+struct StaticKernel {
+    int n = 0;
+    int nstages = 0;
+    int radix[8] = {};
+    int tpt = 0;
+    const void *fn[2][3] = {};  // [forward][C2C, R2C packed, C2R packed]
+};
+const StaticKernel *find_static_kernel(int n);
+cudaError_t fill_stage_twiddles(float2 *t, const int *radix, int nstages, cudaStream_t st);
+int64_t stage_twiddle_count(const int *radix, int nstages);
 // Process-wide device error word of the current device (bounded waits that
 // gave up set it); read and cleared by asdFftSynchronize.
 int *device_error_word(int device);
@@ -48,6 +62,8 @@ struct DeviceTable {
 using TablePtr = std::shared_ptr<DeviceTable>;
 // t[m] = exp(-2 pi i (m*mult mod denom) / denom), m < count
 TablePtr get_table(int64_t count, int64_t denom, int64_t mult, int device, std::string *err);
+// per-stage twiddle tables of a static kernel's radix sequence
+TablePtr get_stage_table(const StaticKernel &k, int device, std::string *err);
 
 enum class Buf : int { kUserIn = 0, kUserOut = 1, kWs0 = 2, kWs1 = 3 };
 
@@ -62,10 +78,12 @@ struct Step {
     Buf src = Buf::kUserIn;
     Buf dst = Buf::kUserOut;
     // optional TMA-pipelined row variant of the same step (used when the
-    // source pointer is 16-byte aligned)
+    // source pointer is 16-byte aligned); row_fn != nullptr selects a
+    // compile-time specialised kernel instead of the runtime-radix one
     bool has_row = false;
     TileDesc rd{};
     int row_grid = 1;
+    const void *row_fn = nullptr;
     // kR2CPost / kC2RPre
     int64_t rows = 0, m = 0, src_dist = 0, dst_dist = 0;
     const float2 *lo = nullptr, *hi = nullptr;
