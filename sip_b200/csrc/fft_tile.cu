@@ -15,6 +15,8 @@
 // The shared-memory row index is padded (i + i/16) so that the strided
 // scatter of the early stages and the column-tile loads are bank-conflict
 // free for 8-byte elements.
+#include <algorithm>
+
 #include "codelets.cuh"
 #include "fft_tile.cuh"
 #include "sipfft_internal.h"
@@ -153,6 +155,34 @@ __device__ __forceinline__ void load_tile(const TileDesc &d, float2 *sm, int64_t
         }
         return;
     }
+    if (io == IO_BLUE_PRE) {
+        const int l = tid / d.tpt, lane = tid % d.tpt;
+        if (l >= ntr) return;
+        const int64_t base = col_base(d.in_a, o, c0 + l);
+        float2 *row = sm + l * P;
+        const int nb = d.blue_n;
+        for (int e = lane; e < n; e += d.tpt) {
+            float2 v = make_float2(0.f, 0.f);
+            if (e < nb) {
+                if (d.blue_kind == 1) {
+                    v = make_float2(static_cast<const float *>(d.in)[base + e], 0.f);
+                } else if (d.blue_kind == 2) {
+                    const float2 *x = static_cast<const float2 *>(d.in) + base;
+                    if (2 * e <= nb) {
+                        v = x[e];
+                        if (e == 0 || 2 * e == nb) v.y = 0.f;
+                    } else {
+                        v = cconj(x[nb - e]);
+                    }
+                } else {
+                    v = static_cast<const float2 *>(d.in)[base + e];
+                }
+                v = cmul(v, __ldg(d.chirp + e));
+            }
+            row[pad(e)] = v;
+        }
+        return;
+    }
     if (io == IO_C2R_FULL) {
         const int l = tid / d.tpt, lane = tid % d.tpt;
         if (l >= ntr) return;
@@ -220,6 +250,24 @@ __device__ __forceinline__ void store_tile(const TileDesc &d, const float2 *sm, 
         }
         return;
     }
+    if (io == IO_BLUE_PRE || io == IO_BLUE_POST) {
+        const int l = tid / d.tpt, lane = tid % d.tpt;
+        if (l >= ntr) return;
+        const int64_t base = col_base(d.out_a, o, c0 + l);
+        const float2 *row = sm + l * P;
+        if (io == IO_BLUE_PRE) {
+            float2 *y = static_cast<float2 *>(d.out) + base;
+            for (int e = lane; e < n; e += d.tpt) y[e] = cmul(row[pad(e)], __ldg(d.bmul + e));
+        } else if (d.blue_kind == 2) {
+            float *y = static_cast<float *>(d.out) + base;
+            for (int e = lane; e < d.blue_n; e += d.tpt) y[e] = cmul(row[pad(e)], __ldg(d.chirp + e)).x;
+        } else {
+            const int count = d.blue_kind == 1 ? d.blue_n / 2 + 1 : d.blue_n;
+            float2 *y = static_cast<float2 *>(d.out) + base;
+            for (int e = lane; e < count; e += d.tpt) y[e] = cmul(row[pad(e)], __ldg(d.chirp + e));
+        }
+        return;
+    }
     const bool contiguous = d.out_a.estride == 1;
     int l, e0, estep;
     if (contiguous) {
@@ -284,6 +332,61 @@ __global__ void twiddle_kernel(float2 *t, int64_t count, int64_t denom, int64_t 
         sincospi(2.0 * static_cast<double>(idx) / static_cast<double>(denom), &s, &c);
         t[m] = make_float2(static_cast<float>(c), static_cast<float>(-s));
     }
+}
+
+// Bluestein tables.  chirp[n] = exp(s*pi*i*(n^2 mod 2N)/N) (s = -1 forward),
+// with n^2 reduced exactly in 64-bit integers before the FP64 evaluation.
+__global__ void chirp_kernel(float2 *t, int64_t n_len, int sign)
+{
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n_len;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t q = (i * i) % (2 * n_len);
+        double s, c;
+        sincospi(static_cast<double>(q) / static_cast<double>(n_len), &s, &c);
+        t[i] = make_float2(static_cast<float>(c), static_cast<float>(sign * s));
+    }
+}
+
+// b[m] = conj(chirp[m]) for m < N, b[M-m] = conj(chirp[m]) for 0 < m < N, else 0
+__global__ void bluestein_b_kernel(float2 *b, const float2 *chirp, int64_t n_len, int64_t m_len)
+{
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < m_len;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        float2 v = make_float2(0.f, 0.f);
+        if (i < n_len)
+            v = cconj(chirp[i]);
+        else if (m_len - i < n_len)
+            v = cconj(chirp[m_len - i]);
+        b[i] = v;
+    }
+}
+
+__global__ void scale_kernel(float2 *b, int64_t count, float s)
+{
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < count;
+         i += int64_t(gridDim.x) * blockDim.x)
+        b[i] = cscale(b[i], s);
+}
+
+cudaError_t fill_chirp(float2 *t, int64_t n_len, bool forward, cudaStream_t st)
+{
+    const int grid = static_cast<int>(std::min<int64_t>((n_len + 255) / 256, 1024));
+    chirp_kernel<<<grid, 256, 0, st>>>(t, n_len, forward ? -1 : 1);
+    return cudaGetLastError();
+}
+
+cudaError_t fill_bluestein_b(float2 *b, const float2 *chirp, int64_t n_len, int64_t m_len, cudaStream_t st)
+{
+    const int grid = static_cast<int>(std::min<int64_t>((m_len + 255) / 256, 1024));
+    bluestein_b_kernel<<<grid, 256, 0, st>>>(b, chirp, n_len, m_len);
+    return cudaGetLastError();
+}
+
+cudaError_t scale_table(float2 *b, int64_t count, float s, cudaStream_t st)
+{
+    const int grid = static_cast<int>(std::min<int64_t>((count + 255) / 256, 1024));
+    scale_kernel<<<grid, 256, 0, st>>>(b, count, s);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------------------------ host side

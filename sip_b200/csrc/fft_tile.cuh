@@ -24,6 +24,10 @@ enum IoKind : int {
     IO_C2R_PACKED = 2,  // n+1 bins; pre-twiddle to n complex; n-point FFT; written as 2n reals
     IO_R2C_FULL = 3,    // odd real length n, zero imaginary part; n-point FFT; bins 0..n/2
     IO_C2R_FULL = 4,    // bins 0..n/2 of odd n, Hermitian extension; n-point FFT; real part
+    // Bluestein (chirp-z) for lengths with prime factors the codelets do not
+    // cover: an N-point transform as a length-M circular convolution.
+    IO_BLUE_PRE = 5,    // a[e] = x[e]*chirp[e] (e < N, else 0); M-point FFT; store A*Bmul
+    IO_BLUE_POST = 6,   // M-point inverse FFT; store chirp[k]*y[k] for the first N (or N/2+1) outputs
 };
 
 // Address of element e of transform (outer o, column c):
@@ -72,6 +76,13 @@ struct TileDesc {
     // occupies (R_s - 1) * Ns_s entries laid out [r-1][k], value
     // exp(-2 pi i r k / (Ns_s R_s)), so a warp's loads for one r are contiguous.
     const float2 *stw;
+    // Bluestein: chirp[e] = exp(s*pi*i*(e^2 mod 2N)/N), bmul = FFT_M(conj chirp)/M,
+    // blue_n = N, blue_kind: 0 complex, 1 real input (pre) / half spectrum
+    // output (post), 2 Hermitian half-spectrum input (pre) / real output (post)
+    const float2 *chirp;
+    const float2 *bmul;
+    int blue_n;
+    int blue_kind;
 };
 
 }  // namespace sipfft

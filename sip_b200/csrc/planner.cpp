@@ -166,6 +166,15 @@ struct Builder {
     bool add_tile(int io, int n, int tw_mul, const float2 *tw, bool column, int64_t n_outer, int64_t n_cols,
                   const Addr &ia, const Addr &oa, Buf src, Buf dst, const std::string &what)
     {
+        Step s;
+        if (!make_tile(s, io, n, tw_mul, tw, column, n_outer, n_cols, ia, oa, src, dst, what)) return false;
+        p.steps.push_back(s);
+        return true;
+    }
+
+    bool make_tile(Step &s, int io, int n, int tw_mul, const float2 *tw, bool column, int64_t n_outer,
+                   int64_t n_cols, const Addr &ia, const Addr &oa, Buf src, Buf dst, const std::string &what)
+    {
         std::vector<int> radices;
         if (!factor_radices(n, radices)) {
             err = "length " + std::to_string(n) + " has a prime factor above 13";
@@ -173,7 +182,7 @@ struct Builder {
         }
         TileCfg c;
         if (!choose_cfg(n, column, n_cols, c, err)) return false;
-        Step s;
+        s = Step();
         s.kind = StepKind::kTile;
         s.forward = fwd;
         s.src = src;
@@ -200,7 +209,6 @@ struct Builder {
         if (!column && n_outer == 1 && ia.estride == 1 && oa.estride == 1 &&
             (io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
             add_row_variant(s, c, ia.cstride, oa.cstride);
-        p.steps.push_back(s);
         return true;
     }
 
@@ -308,6 +316,73 @@ struct Builder {
         return true;
     }
 
+    // Bluestein (chirp-z) N-point transform of contiguous rows for lengths
+    // whose prime factors the codelets do not cover: a length-M circular
+    // convolution (M = 2^k >= 2N-1) done as two M-point FFT launches with the
+    // chirp pre/post multiplies and the precomputed FFT of the chirp fused in.
+    // kind: 0 C2C, 1 R2C (real in, N/2+1 out), 2 C2R (N/2+1 in, real out).
+    bool add_bluestein(int kind, int64_t n, int64_t rows, int64_t in_dist, int64_t out_dist, Buf src, Buf dst)
+    {
+        int64_t m = 1;
+        while (m < 2 * n - 1) m *= 2;
+        if (m > kMaxRowN) {
+            err = "length " + std::to_string(n) + " needs Bluestein with M > " + std::to_string(kMaxRowN);
+            return false;
+        }
+        auto chirp = std::make_shared<DeviceTable>();
+        auto bmul = std::make_shared<DeviceTable>();
+        chirp->device = bmul->device = device;
+        chirp->count = n;
+        bmul->count = m;
+        cudaError_t e = cudaMalloc(&chirp->ptr, sizeof(float2) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&bmul->ptr, sizeof(float2) * m);
+        if (e == cudaSuccess) e = fill_chirp(chirp->ptr, n, fwd, 0);
+        if (e == cudaSuccess) e = fill_bluestein_b(bmul->ptr, chirp->ptr, n, m, 0);
+        const float2 *twm = table(m, m);
+        if (!twm) return false;
+        if (e == cudaSuccess) {
+            // FFT_M of b in place (one row, forward), then fold in the 1/M of the inverse
+            Step tmp;
+            if (!make_tile(tmp, IO_C2C, static_cast<int>(m), 1, twm, false, 1, 1, Addr{0, m, 1, 0, 0},
+                           Addr{0, m, 1, 0, 0}, Buf::kUserIn, Buf::kUserOut, "bluestein table"))
+                return false;
+            tmp.d.in = bmul->ptr;
+            tmp.d.out = bmul->ptr;
+            e = launch_tile(tmp.d, tmp.maxe, true, tmp.grid, 0);
+        }
+        if (e == cudaSuccess) e = scale_table(bmul->ptr, m, 1.0f / static_cast<float>(m), 0);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+        if (e != cudaSuccess) {
+            err = std::string("twiddle table: ") + cudaGetErrorString(e);
+            cudaGetLastError();
+            return false;
+        }
+        p.tables.push_back(chirp);
+        p.tables.push_back(bmul);
+        Buf ws = other_ws(src, dst);
+        need_ws(ws, size_t(rows) * m * sizeof(float2));
+        std::ostringstream w;
+        w << "Bluestein n=" << n << " via M=" << m << " rows=" << rows;
+        Step s1, s2;
+        if (!make_tile(s1, IO_BLUE_PRE, static_cast<int>(m), 1, twm, false, 1, rows, Addr{0, in_dist, 1, 0, 0},
+                       Addr{0, m, 1, 0, 0}, src, ws, w.str() + " (chirp, FFT, multiply)"))
+            return false;
+        if (!make_tile(s2, IO_BLUE_POST, static_cast<int>(m), 1, twm, false, 1, rows, Addr{0, m, 1, 0, 0},
+                       Addr{0, out_dist, 1, 0, 0}, ws, dst, w.str() + " (inverse FFT, chirp)"))
+            return false;
+        for (Step *st : {&s1, &s2}) {
+            st->d.chirp = chirp->ptr;
+            st->d.bmul = bmul->ptr;
+            st->d.blue_n = static_cast<int>(n);
+            st->d.blue_kind = kind;
+        }
+        s1.forward = true;
+        s2.forward = false;
+        p.steps.push_back(s1);
+        p.steps.push_back(s2);
+        return true;
+    }
+
     // C2C along one axis of a contiguous tensor viewed as [outer][n][inner].
     bool axis_c2c(int64_t n, int64_t outer, int64_t inner, Buf src, Buf dst)
     {
@@ -318,6 +393,9 @@ struct Builder {
         }
         std::ostringstream w;
         w << "C2C axis n=" << n << " outer=" << outer << " inner=" << inner;
+        std::vector<int> probe;
+        const bool smooth = factor_radices(n, probe);
+        if (inner == 1 && !smooth) return add_bluestein(0, n, outer, n, n, src, dst);
         if (inner == 1) {
             if (n <= kMaxRowN) {
                 const float2 *tw = table(n, n);
@@ -351,6 +429,8 @@ struct Builder {
     bool rows_r2c(int64_t n, int64_t rows, Buf src, Buf dst)
     {
         const int64_t h = n / 2 + 1;
+        std::vector<int> probe;
+        if (!factor_radices(n % 2 == 0 ? n / 2 : n, probe)) return add_bluestein(1, n, rows, n, h, src, dst);
         std::ostringstream w;
         w << "R2C rows n=" << n << " rows=" << rows;
         if (n % 2 == 0 && n / 2 <= kMaxRowN) {
@@ -396,6 +476,8 @@ struct Builder {
     bool rows_c2r(int64_t n, int64_t rows, Buf src, Buf dst)
     {
         const int64_t h = n / 2 + 1;
+        std::vector<int> probe;
+        if (!factor_radices(n % 2 == 0 ? n / 2 : n, probe)) return add_bluestein(2, n, rows, h, n, src, dst);
         std::ostringstream w;
         w << "C2R rows n=" << n << " rows=" << rows;
         if (n % 2 == 0 && n / 2 <= kMaxRowN) {

@@ -20,6 +20,9 @@ constexpr int kB200Sms = 148;
 
 cudaError_t launch_tile(const TileDesc &d, int maxe, bool forward, int grid, cudaStream_t st);
 cudaError_t fill_twiddles(float2 *t, int64_t count, int64_t denom, int64_t mult, cudaStream_t st);
+cudaError_t fill_chirp(float2 *t, int64_t n_len, bool forward, cudaStream_t st);
+cudaError_t fill_bluestein_b(float2 *b, const float2 *chirp, int64_t n_len, int64_t m_len, cudaStream_t st);
+cudaError_t scale_table(float2 *b, int64_t count, float s, cudaStream_t st);
 // TMA-pipelined persistent kernel for contiguous rows (row_fft.cu).  The row
 // descriptor keeps the row distance in in_a.dist / out_a.dist and the
 // per-buffer float2 count in g_ns.

@@ -74,7 +74,9 @@ def check(sizes, typ, fwd, batch, seed=0, vertical=False):
 
 
 C2C_SIZES = [1, 2, 3, 4, 5, 7, 8, 11, 13, 16, 30, 64, 100, 128, 143, 210, 256, 343, 512, 1000, 1024, 1500,
-             2048, 3000, 4096, 6561, 8192, 10000, 15000, 16384, 24576, 32768, 65536, 3 * 2 ** 15, 2 ** 20]
+             2048, 3000, 4096, 6561, 8192, 10000, 15000, 16384, 24576, 32768, 65536, 3 * 2 ** 15, 2 ** 20,
+             # prime factors above 13: Bluestein
+             17, 31, 97, 202, 1021, 4099, 8191]
 
 
 @pytest.mark.parametrize("n", C2C_SIZES)
@@ -85,7 +87,9 @@ def test_c2c_1d(cuda, n, fwd):
 
 
 REAL_SIZES = [1, 2, 3, 4, 5, 6, 7, 30, 64, 100, 243, 256, 1000, 1024, 3000, 4096, 8192, 15625, 16384,
-              30000, 65536, 131072]
+              30000, 65536, 131072,
+              # prime factors above 13 (Bluestein): odd, even, and even with an odd large half
+              17, 31, 34, 1021, 2042]
 
 
 @pytest.mark.parametrize("n", REAL_SIZES)
@@ -204,9 +208,9 @@ def test_exec_error_paths(cuda):
     y = torch.zeros((1, 65536), dtype=torch.complex64, device="cuda")
     assert fft.load_library().asdFftExecRaw(h, y.data_ptr(), y.data_ptr()) == fft.ACL_ERROR_INTERNAL_ERROR
     assert fft.asdFftDestroy(h) == fft.ACL_SUCCESS
-    # unsupported length (prime factor 17) is refused at plan time, not at run time
+    # an unsupported length (large prime beyond the Bluestein range) is refused at plan time
     h = fft.asdFftCreate()
-    assert fft.asdFftMakePlan1D(h, 17 * 19, C2C, FWD, 1) == fft.ACL_ERROR_API_NOT_SUPPORT
+    assert fft.asdFftMakePlan1D(h, 65537, C2C, FWD, 1) == fft.ACL_ERROR_API_NOT_SUPPORT
     fft.asdFftDestroy(h)
 
 
