@@ -25,6 +25,26 @@ ASDSIP_API int64_t asdFftDescribePlan(void *handle, char *buf, int64_t len);
 /* Number of kernel launches one execution of the plan issues. */
 ASDSIP_API int32_t asdFftPlanLaunchCount(void *handle);
 
+/* ---- uneven batches: many 1D C2C groups (length sizes[i], count batches[i]) stored back to back,
+ * executed by ONE persistent kernel launch (optionally replayed from a captured CUDA graph).
+ * tune_cache: optional path of the autotuner's cache (choices for this GPU are loaded). */
+ASDSIP_API int32_t asdFftBatchPlanCreate(void **plan, const int64_t *sizes, const int64_t *batches, int32_t ngroups,
+                                         int32_t direction, const char *tune_cache);
+ASDSIP_API int32_t asdFftBatchGetWorkspaceSize(void *plan, size_t *bytes);
+/* in != out; workspace of GetWorkspaceSize bytes; stream = cudaStream_t; use_graph != 0 captures once and
+ * replays while (in, out, workspace, stream) stay the same. */
+ASDSIP_API int32_t asdFftBatchExec(void *plan, const void *input, void *output, void *workspace, void *stream,
+                                   int32_t use_graph);
+ASDSIP_API int32_t asdFftBatchPlanDestroy(void *plan);
+ASDSIP_API int64_t asdFftBatchDescribe(void *plan, char *buf, int64_t len);
+
+/* ---- autotuner: times radix orders and elements per thread for each length (rows[i] transforms, capped at 256)
+ * and keeps the fastest per length; cache_path (optional) receives one JSON object per line keyed by
+ * GPU name, type, precision and length.  TuneCacheLoad returns the number of entries loaded for this GPU. */
+ASDSIP_API int32_t asdFftAutotune(const int64_t *sizes, const int64_t *rows, int32_t n, int32_t direction,
+                                  const char *cache_path);
+ASDSIP_API int32_t asdFftTuneCacheLoad(const char *cache_path);
+
 #ifdef __cplusplus
 }
 #endif

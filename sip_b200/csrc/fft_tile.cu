@@ -128,7 +128,8 @@ __device__ __forceinline__ float2 pass_twiddle(const TileDesc &d, int64_t e, int
 
 // ------------------------------------------------------------------------------------ load
 template <bool FWD>
-__device__ __forceinline__ void load_tile(const TileDesc &d, float2 *sm, int64_t o, int64_t c0, int ntr)
+__device__ __forceinline__ void load_tile(const TileDesc &d, const void *in, float2 *sm, int64_t o, int64_t c0,
+                                          int ntr)
 {
     const int tid = threadIdx.x, bd = blockDim.x;
     const int n = d.n, P = d.pitch;
@@ -137,7 +138,7 @@ __device__ __forceinline__ void load_tile(const TileDesc &d, float2 *sm, int64_t
         // pairs (k, n-k) of the half spectrum -> packed n-point input
         const int l = tid / d.tpt, lane = tid % d.tpt;
         if (l >= ntr) return;
-        const float2 *x = static_cast<const float2 *>(d.in) + col_base(d.in_a, o, c0 + l);
+        const float2 *x = static_cast<const float2 *>(in) + col_base(d.in_a, o, c0 + l);
         float2 *row = sm + l * P;
         for (int k = lane; 2 * k <= n; k += d.tpt) {
             float2 xk = x[k];
@@ -165,9 +166,9 @@ __device__ __forceinline__ void load_tile(const TileDesc &d, float2 *sm, int64_t
             float2 v = make_float2(0.f, 0.f);
             if (e < nb) {
                 if (d.blue_kind == 1) {
-                    v = make_float2(static_cast<const float *>(d.in)[base + e], 0.f);
+                    v = make_float2(static_cast<const float *>(in)[base + e], 0.f);
                 } else if (d.blue_kind == 2) {
-                    const float2 *x = static_cast<const float2 *>(d.in) + base;
+                    const float2 *x = static_cast<const float2 *>(in) + base;
                     if (2 * e <= nb) {
                         v = x[e];
                         if (e == 0 || 2 * e == nb) v.y = 0.f;
@@ -175,7 +176,7 @@ __device__ __forceinline__ void load_tile(const TileDesc &d, float2 *sm, int64_t
                         v = cconj(x[nb - e]);
                     }
                 } else {
-                    v = static_cast<const float2 *>(d.in)[base + e];
+                    v = static_cast<const float2 *>(in)[base + e];
                 }
                 v = cmul(v, __ldg(d.chirp + e));
             }
@@ -186,7 +187,7 @@ __device__ __forceinline__ void load_tile(const TileDesc &d, float2 *sm, int64_t
     if (io == IO_C2R_FULL) {
         const int l = tid / d.tpt, lane = tid % d.tpt;
         if (l >= ntr) return;
-        const float2 *x = static_cast<const float2 *>(d.in) + col_base(d.in_a, o, c0 + l);
+        const float2 *x = static_cast<const float2 *>(in) + col_base(d.in_a, o, c0 + l);
         float2 *row = sm + l * P;
         for (int k = lane; 2 * k <= n; k += d.tpt) {
             float2 xk = x[k];
@@ -213,11 +214,11 @@ __device__ __forceinline__ void load_tile(const TileDesc &d, float2 *sm, int64_t
     const int64_t es = d.in_a.estride;
     float2 *row = sm + l * P;
     if (io == IO_R2C_FULL) {
-        const float *x = static_cast<const float *>(d.in) + base;
+        const float *x = static_cast<const float *>(in) + base;
         for (int e = e0; e < n; e += estep) row[pad(e)] = make_float2(x[e * es], 0.f);
         return;
     }
-    const float2 *x = static_cast<const float2 *>(d.in) + base;
+    const float2 *x = static_cast<const float2 *>(in) + base;
     if (d.g_twiddle) {
         const int64_t kc = (c0 + l) % d.g_ns;
         for (int e = e0; e < n; e += estep) row[pad(e)] = cmul(x[e * es], pass_twiddle<FWD>(d, e, kc));
@@ -228,7 +229,8 @@ __device__ __forceinline__ void load_tile(const TileDesc &d, float2 *sm, int64_t
 
 // ------------------------------------------------------------------------------------ store
 template <bool FWD>
-__device__ __forceinline__ void store_tile(const TileDesc &d, const float2 *sm, int64_t o, int64_t c0, int ntr)
+__device__ __forceinline__ void store_tile(const TileDesc &d, void *out, const float2 *sm, int64_t o, int64_t c0,
+                                           int ntr)
 {
     const int tid = threadIdx.x, bd = blockDim.x;
     const int n = d.n, P = d.pitch;
@@ -236,7 +238,7 @@ __device__ __forceinline__ void store_tile(const TileDesc &d, const float2 *sm, 
     if (io == IO_R2C_PACKED) {
         const int l = tid / d.tpt, lane = tid % d.tpt;
         if (l >= ntr) return;
-        float2 *y = static_cast<float2 *>(d.out) + col_base(d.out_a, o, c0 + l);
+        float2 *y = static_cast<float2 *>(out) + col_base(d.out_a, o, c0 + l);
         const float2 *row = sm + l * P;
         for (int k = lane; 2 * k <= n; k += d.tpt) {
             const float2 zk = row[pad(k)];
@@ -256,14 +258,14 @@ __device__ __forceinline__ void store_tile(const TileDesc &d, const float2 *sm, 
         const int64_t base = col_base(d.out_a, o, c0 + l);
         const float2 *row = sm + l * P;
         if (io == IO_BLUE_PRE) {
-            float2 *y = static_cast<float2 *>(d.out) + base;
+            float2 *y = static_cast<float2 *>(out) + base;
             for (int e = lane; e < n; e += d.tpt) y[e] = cmul(row[pad(e)], __ldg(d.bmul + e));
         } else if (d.blue_kind == 2) {
-            float *y = static_cast<float *>(d.out) + base;
+            float *y = static_cast<float *>(out) + base;
             for (int e = lane; e < d.blue_n; e += d.tpt) y[e] = cmul(row[pad(e)], __ldg(d.chirp + e)).x;
         } else {
             const int count = d.blue_kind == 1 ? d.blue_n / 2 + 1 : d.blue_n;
-            float2 *y = static_cast<float2 *>(d.out) + base;
+            float2 *y = static_cast<float2 *>(out) + base;
             for (int e = lane; e < count; e += d.tpt) y[e] = cmul(row[pad(e)], __ldg(d.chirp + e));
         }
         return;
@@ -284,19 +286,20 @@ __device__ __forceinline__ void store_tile(const TileDesc &d, const float2 *sm, 
     const int64_t es = d.out_a.estride;
     const float2 *row = sm + l * P;
     if (io == IO_C2R_FULL) {
-        float *y = static_cast<float *>(d.out) + base;
+        float *y = static_cast<float *>(out) + base;
         for (int e = e0; e < n; e += estep) y[e * es] = row[pad(e)].x;
         return;
     }
     const int count = (io == IO_R2C_FULL) ? n / 2 + 1 : n;
-    float2 *y = static_cast<float2 *>(d.out) + base;
+    float2 *y = static_cast<float2 *>(out) + base;
     for (int e = e0; e < count; e += estep) y[e * es] = row[pad(e)];
 }
 
+// One tile: load, Stockham stages, store.  Threads beyond tb*tpt (a launch
+// shared by tiles of different shapes) only take part in the barriers.
 template <int MAXE, bool FWD>
-__global__ void __launch_bounds__(512, 1) tile_fft_kernel(const __grid_constant__ TileDesc d)
+__device__ __forceinline__ void process_tile(const TileDesc &d, const void *in, void *out, int64_t g, float2 *sm)
 {
-    extern __shared__ float2 sm[];
     const int tid = threadIdx.x;
     int l, lane;
     if (d.xfast) {
@@ -306,16 +309,79 @@ __global__ void __launch_bounds__(512, 1) tile_fft_kernel(const __grid_constant_
         l = tid / d.tpt;
         lane = tid % d.tpt;
     }
-    for (int64_t g = blockIdx.x; g < d.num_tiles; g += gridDim.x) {
-        const int64_t o = g / d.tiles_per_outer;
-        const int64_t c0 = (g % d.tiles_per_outer) * d.tb;
-        const int64_t left = d.n_cols - c0;
-        const int ntr = left < d.tb ? static_cast<int>(left) : d.tb;
-        load_tile<FWD>(d, sm, o, c0, ntr);
+    const bool thread_on = tid < d.tb * d.tpt;
+    const int64_t o = g / d.tiles_per_outer;
+    const int64_t c0 = (g % d.tiles_per_outer) * d.tb;
+    const int64_t left = d.n_cols - c0;
+    const int ntr = left < d.tb ? static_cast<int>(left) : d.tb;
+    load_tile<FWD>(d, in, sm, o, c0, ntr);
+    __syncthreads();
+    run_stages<MAXE, FWD>(sm + (thread_on ? l : 0) * d.pitch, d, lane, thread_on && l < ntr);
+    store_tile<FWD>(d, out, sm, o, c0, ntr);
+    __syncthreads();
+}
+
+template <int MAXE, bool FWD>
+__global__ void __launch_bounds__(512, 1) tile_fft_kernel(const __grid_constant__ TileDesc d)
+{
+    extern __shared__ float2 sm[];
+    for (int64_t g = blockIdx.x; g < d.num_tiles; g += gridDim.x) process_tile<MAXE, FWD>(d, d.in, d.out, g, sm);
+}
+
+// ------------------------------------------------------------------------------------ uneven batches
+// One persistent launch over many transform groups of different lengths.
+// Work items (segment, tile) are dequeued in order from a global counter;
+// a segment that consumes another segment's output (the next pass of a
+// multi-pass transform, the second half of a Bluestein transform) waits,
+// with a bounded spin, until every tile of that segment has been published.
+// Items are ordered so that every producer tile is dequeued before its
+// consumers and all CTAs are resident (grid = occupancy), so the waits end.
+template <int MAXE>
+__global__ void __launch_bounds__(512, 1)
+    batch_fft_kernel(const BatchSeg *__restrict__ segs, const int2 *__restrict__ items, int nitems, int *counter,
+                     int *done, BatchBufs bufs, int *err)
+{
+    extern __shared__ float2 sm[];
+    __shared__ int s_item;
+    __shared__ int s_ok;
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(counter, 1);
         __syncthreads();
-        run_stages<MAXE, FWD>(sm + l * d.pitch, d, lane, l < ntr);
-        store_tile<FWD>(d, sm, o, c0, ntr);
+        const int w = s_item;
         __syncthreads();
+        if (w >= nitems) break;
+        const int2 it = items[w];
+        const BatchSeg &sg = segs[it.x];
+        if (sg.dep >= 0) {
+            if (tid == 0) {
+                const int need = segs[sg.dep].ntiles;
+                int ok = 0;
+                for (uint32_t poll = 0; poll < (1u << 24); poll++) {
+                    int v;
+                    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(done + sg.dep) : "memory");
+                    if (v >= need) {
+                        ok = 1;
+                        break;
+                    }
+                    __nanosleep(128);
+                }
+                if (!ok) atomicExch(err, 2);
+                s_ok = ok;
+            }
+            __syncthreads();
+            if (!s_ok) continue;  // give up on this item; the error word reports it
+        }
+        const char *in = static_cast<const char *>(bufs.p[sg.in_buf]) + sg.in_off;
+        char *out = static_cast<char *>(bufs.p[sg.out_buf]) + sg.out_off;
+        if (sg.fwd)
+            process_tile<MAXE, true>(sg.d, in, out, it.y, sm);
+        else
+            process_tile<MAXE, false>(sg.d, in, out, it.y, sm);
+        if (tid == 0) {
+            __threadfence();
+            atomicAdd(done + it.x, 1);
+        }
     }
 }
 
@@ -417,6 +483,23 @@ cudaError_t launch_tile(const TileDesc &d, int maxe, bool forward, int grid, cud
     if (maxe <= 16) return forward ? launch_one<16, true>(d, grid, block, smem, st)
                                    : launch_one<16, false>(d, grid, block, smem, st);
     return forward ? launch_one<32, true>(d, grid, block, smem, st) : launch_one<32, false>(d, grid, block, smem, st);
+}
+
+const void *batch_kernel_fn() { return reinterpret_cast<const void *>(batch_fft_kernel<32>); }
+
+cudaError_t launch_batch(int grid, int block, size_t smem, const BatchSeg *segs, const int2 *items, int nitems,
+                         int *counter, int *done, const BatchBufs &bufs, int *err, cudaStream_t st)
+{
+    const void *fn = batch_kernel_fn();
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBytes);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    BatchBufs b = bufs;
+    void *args[] = {&segs, &items, &nitems, &counter, &done, &b, &err};
+    return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, smem, st);
 }
 
 cudaError_t fill_twiddles(float2 *t, int64_t count, int64_t denom, int64_t mult, cudaStream_t st)

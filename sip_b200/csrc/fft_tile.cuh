@@ -85,4 +85,22 @@ struct TileDesc {
     int blue_kind;
 };
 
+// One segment of an uneven batch: a tile-kernel step whose source and
+// destination are byte offsets into one of four buffers (user input, user
+// output, workspace slot 0 / 1).
+struct BatchSeg {
+    TileDesc d;
+    int64_t in_off;
+    int64_t out_off;
+    int in_buf;
+    int out_buf;
+    int dep;     // segment whose output this one reads, -1 if none
+    int ntiles;
+    int fwd;     // direction of this segment's FFT
+};
+
+struct BatchBufs {
+    void *p[4];
+};
+
 }  // namespace sipfft

@@ -19,6 +19,8 @@
 
 namespace sipfft {
 
+bool valid_radices(const std::vector<int> &r, int64_t n);
+
 namespace {
 
 constexpr int64_t kMaxRowN = 16384;        // longest single-CTA transform: 512 threads x 32 points
@@ -50,13 +52,17 @@ struct TileCfg {
 };
 
 // Threads, transforms per CTA and shared-memory pitch for one tile launch.
-bool choose_cfg(int n, bool column, int64_t ncols, TileCfg &c, std::string &err)
+bool choose_cfg(int n, bool column, int64_t ncols, TileCfg &c, std::string &err, int maxe_override = 0,
+                int row_threads = kRowThreadsTarget, int row_smem = kRowSmemTarget)
 {
     if (n < 1 || n > 32768) {
         err = "transform length out of the single-CTA range";
         return false;
     }
     c.maxe = n <= 4096 ? 16 : 32;
+    if (maxe_override == 8 || maxe_override == 16 || maxe_override == 32) {
+        if ((n + maxe_override - 1) / maxe_override <= kMaxThreads) c.maxe = maxe_override;
+    }
     c.tpt = std::max(1, (n + c.maxe - 1) / c.maxe);
     if (c.tpt > kMaxThreads) {
         err = "too many threads per transform";
@@ -73,8 +79,8 @@ bool choose_cfg(int n, bool column, int64_t ncols, TileCfg &c, std::string &err)
             }
         }
     } else {
-        int tb = std::max(1, kRowThreadsTarget / c.tpt);
-        while (tb > 1 && tb * bytes_per > kRowSmemTarget) tb /= 2;
+        int tb = std::max(1, row_threads / c.tpt);
+        while (tb > 1 && tb * bytes_per > row_smem) tb /= 2;
         if (tb > ncols) tb = static_cast<int>(std::max<int64_t>(1, ncols));
         while (tb > 1 && tb * c.tpt > kMaxThreads) tb /= 2;
         c.tb = (bytes_per <= kMaxSmemBytes) ? tb : 0;
@@ -180,8 +186,14 @@ struct Builder {
             err = "length " + std::to_string(n) + " has a prime factor above 13";
             return false;
         }
+        int maxe_override = 0;
+        TuneChoice tc;
+        if (p.use_tuned && tuned_choice(n, tc) && valid_radices(tc.radices, n)) {
+            radices = tc.radices;
+            maxe_override = tc.maxe;
+        }
         TileCfg c;
-        if (!choose_cfg(n, column, n_cols, c, err)) return false;
+        if (!choose_cfg(n, column, n_cols, c, err, maxe_override, p.row_threads, p.row_smem)) return false;
         s = Step();
         s.kind = StepKind::kTile;
         s.forward = fwd;
@@ -533,6 +545,16 @@ std::string finish(Plan &p, Builder &b, bool ok)
 }
 
 }  // namespace
+
+bool valid_radices(const std::vector<int> &r, int64_t n)
+{
+    int64_t prod = 1;
+    for (int x : r) {
+        if (x != 2 && x != 3 && x != 4 && x != 5 && x != 7 && x != 8 && x != 11 && x != 13 && x != 16) return false;
+        prod *= x;
+    }
+    return prod == n && r.size() <= static_cast<size_t>(kMaxStages);
+}
 
 bool factor_radices(int64_t n, std::vector<int> &radices)
 {

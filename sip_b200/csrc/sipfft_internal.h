@@ -30,6 +30,10 @@ cudaError_t launch_row_tiles(const TileDesc &d, int maxe, bool forward, int grid
 size_t row_kernel_smem(const TileDesc &d);
 int row_kernel_blocks_per_sm(const TileDesc &d, int maxe, bool forward);
 int kernel_blocks_per_sm(const void *fn, int threads, size_t smem);
+// persistent uneven-batch kernel (fft_tile.cu)
+const void *batch_kernel_fn();
+cudaError_t launch_batch(int grid, int block, size_t smem, const BatchSeg *segs, const int2 *items, int nitems,
+                         int *counter, int *done, const BatchBufs &bufs, int *err, cudaStream_t st);
 cudaError_t launch_kernel_fn(const void *fn, const TileDesc &d, int grid, size_t smem, int *err, cudaStream_t st);
 
 // Compile-time specialised pipelined row kernels (static_fft.cu).
@@ -94,6 +98,13 @@ struct Step {
     std::string what;  // human-readable description (plan dump)
 };
 
+// Autotuned choice for one length: radix order and elements per thread.
+struct TuneChoice {
+    std::vector<int> radices;
+    int maxe = 0;
+    double us = 0.0;
+};
+
 struct Plan {
     // reference FFTPlan fields (core/fft/fftplan/include/fftplan/fft_plan.h:49-70)
     int fft_type = 0;
@@ -113,8 +124,17 @@ struct Plan {
     size_t ws_bytes = 0;
     std::vector<TablePtr> tables;
     std::mutex mu;
+    bool use_tuned = false;  // consult the autotuner's choices (uneven-batch plans)
+    int row_threads = 256;   // threads per CTA the row tiles aim for
+    int row_smem = 64 * 1024;  // shared memory per CTA the row tiles stay under
     bool forward() const;
 };
+
+// Process-wide autotuner choices keyed by (transform length); see tuner.cpp.
+bool tuned_choice(int64_t n, TuneChoice &out);
+void set_tuned_choice(int64_t n, const TuneChoice &c);
+int load_tune_cache(const std::string &path, int device);
+bool save_tune_cache(const std::string &path, int device);
 
 // Planner entry points (planner.cpp).  They fill plan.steps / ws sizes and
 // return an empty string on success, else the reason.
@@ -127,5 +147,7 @@ std::string describe_plan(const Plan &p);
 
 // Radix decomposition used by the tile kernel (largest radices first).
 bool factor_radices(int64_t n, std::vector<int> &radices);
+// true when every radix has a codelet in the runtime engine and they multiply to n
+bool valid_radices(const std::vector<int> &r, int64_t n);
 
 }  // namespace sipfft

@@ -56,6 +56,8 @@ EXPORTED_SYMBOLS = (
     "asdFftMakePlan2D", "asdFftMakePlan3D", "asdFftGetWorkspaceSize", "asdFftSetWorkspace",
     "asdFftSynchronize", "asdFftGetType",
     "asdFftExecRaw", "asdFftDescribePlan", "asdFftPlanLaunchCount",
+    "asdFftBatchPlanCreate", "asdFftBatchGetWorkspaceSize", "asdFftBatchExec", "asdFftBatchPlanDestroy",
+    "asdFftBatchDescribe", "asdFftAutotune", "asdFftTuneCacheLoad",
 )
 
 
@@ -104,6 +106,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "asdFftExecRaw": (i32, [vp, vp, vp]),
         "asdFftDescribePlan": (i64, [vp, ctypes.c_char_p, i64]),
         "asdFftPlanLaunchCount": (i32, [vp]),
+        "asdFftBatchPlanCreate": (i32, [ctypes.POINTER(vp), P64, P64, i32, i32, ctypes.c_char_p]),
+        "asdFftBatchGetWorkspaceSize": (i32, [vp, ctypes.POINTER(sz)]),
+        "asdFftBatchExec": (i32, [vp, vp, vp, vp, vp, i32]),
+        "asdFftBatchPlanDestroy": (i32, [vp]),
+        "asdFftBatchDescribe": (i64, [vp, ctypes.c_char_p, i64]),
+        "asdFftAutotune": (i32, [P64, P64, i32, i32, ctypes.c_char_p]),
+        "asdFftTuneCacheLoad": (i32, [ctypes.c_char_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -309,3 +318,71 @@ class FftPlan:
             self.close()
         except Exception:
             pass
+
+
+# --- uneven batches (one persistent launch) and the autotuner ------------------------------------
+class BatchPlan:
+    """Groups (length, count) of 1D C2C transforms stored back to back, run by one persistent launch."""
+
+    def __init__(self, groups, direction=ASCEND_FFT_FORWARD, tune_cache: Optional[str] = None):
+        import torch
+
+        lib = load_library()
+        self.groups = [(int(n), int(b)) for n, b in groups]
+        sizes = (ctypes.c_int64 * len(self.groups))(*[n for n, _ in self.groups])
+        batches = (ctypes.c_int64 * len(self.groups))(*[b for _, b in self.groups])
+        h = ctypes.c_void_p()
+        st = lib.asdFftBatchPlanCreate(ctypes.byref(h), sizes, batches, len(self.groups), direction,
+                                       tune_cache.encode() if tune_cache else None)
+        if st != ACL_SUCCESS:
+            raise FftError("asdFftBatchPlanCreate", st)
+        self.handle = h.value
+        n = ctypes.c_size_t(0)
+        lib.asdFftBatchGetWorkspaceSize(self.handle, ctypes.byref(n))
+        self.workspace_bytes = n.value
+        self.workspace = torch.empty(max(1, n.value), dtype=torch.uint8, device="cuda")
+        self.total = sum(n * b for n, b in self.groups)
+        self.offsets = []
+        off = 0
+        for n_, b in self.groups:
+            self.offsets.append(off)
+            off += n_ * b
+
+    def __call__(self, inp, out, stream=None, use_graph=True):
+        import torch
+
+        s = stream if stream is not None else torch.cuda.current_stream()
+        st = load_library().asdFftBatchExec(self.handle, inp.data_ptr(), out.data_ptr(), self.workspace.data_ptr(),
+                                            ctypes.c_void_p(s.cuda_stream), 1 if use_graph else 0)
+        if st != ACL_SUCCESS:
+            raise FftError("asdFftBatchExec", st)
+        return out
+
+    def describe(self) -> str:
+        lib = load_library()
+        n = lib.asdFftBatchDescribe(self.handle, None, 0)
+        buf = ctypes.create_string_buffer(int(n))
+        lib.asdFftBatchDescribe(self.handle, buf, n)
+        return buf.value.decode()
+
+    def close(self):
+        if self.handle:
+            load_library().asdFftBatchPlanDestroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(groups, direction=ASCEND_FFT_FORWARD, cache_path: Optional[str] = None) -> int:
+    lib = load_library()
+    sizes = (ctypes.c_int64 * len(groups))(*[int(n) for n, _ in groups])
+    rows = (ctypes.c_int64 * len(groups))(*[int(b) for _, b in groups])
+    return lib.asdFftAutotune(sizes, rows, len(groups), direction, cache_path.encode() if cache_path else None)
+
+
+def tune_cache_load(cache_path: str) -> int:
+    return load_library().asdFftTuneCacheLoad(cache_path.encode())
