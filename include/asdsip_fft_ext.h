@@ -45,6 +45,26 @@ ASDSIP_API int32_t asdFftAutotune(const int64_t *sizes, const int64_t *rows, int
                                   const char *cache_path);
 ASDSIP_API int32_t asdFftTuneCacheLoad(const char *cache_path);
 
+/* ---- continuous-batching server: requests (type C2C 0x10 or R2C 0x12, direction, length n, rows) are
+ * admitted by a byte budget onto `lanes` CUDA streams with resident plans (one per class, sized for
+ * max_rows) and resident staging buffers; same-class requests that are pending when a lane frees up are
+ * batched into one launch.  device_io != 0: request buffers are device pointers, else host (pinned). */
+ASDSIP_API int32_t asdFftServerCreate(void **server, int64_t budget_bytes, int32_t lanes, int64_t max_rows,
+                                      int32_t device_io);
+ASDSIP_API int32_t asdFftServerWarm(void *server, int32_t type, int32_t direction, int64_t n);
+/* Returns the request id (>= 0) or -1. */
+ASDSIP_API int64_t asdFftServerSubmit(void *server, int32_t type, int32_t direction, int64_t n, int64_t rows,
+                                      const void *input, void *output);
+/* Waits for every submitted request; writes up to cap (id, latency in seconds; < 0 = failed). */
+ASDSIP_API int64_t asdFftServerDrain(void *server, int64_t *ids, double *latency_s, int64_t cap);
+ASDSIP_API int64_t asdFftServerBatches(void *server);
+ASDSIP_API int32_t asdFftServerDestroy(void *server);
+/* Poisson load generator over per-class input/output pools; returns wall seconds (< 0 on error). */
+ASDSIP_API double asdFftServeRun(void *server, double rate, int64_t count, uint64_t seed, int32_t nclasses,
+                                 const int32_t *types, const int64_t *sizes, const void *const *pool_in,
+                                 void *const *pool_out, int64_t rows_min, int64_t rows_max, int32_t direction,
+                                 double *latency_s, int64_t *rows_out, int32_t *class_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -319,7 +319,7 @@ std::string build_batch(BatchPlan &bp)
         p.device = bp.device;
         p.use_tuned = true;
         p.row_threads = 512;
-        p.row_smem = kMaxSmemBytes;
+        p.row_smem = 160 * 1024;  // leaves room for the kernel's static shared memory
         std::string e = build_plan_1d(p);
         if (!e.empty()) return "length " + std::to_string(n) + ": " + e;
         const size_t ws0 = (p.ws_buf_bytes[0] + 255) / 256 * 256;

@@ -8,6 +8,7 @@
 // from the caller's workspace).  Here the tables are generated directly on the
 // GPU in FP64 and rounded to FP32, and intermediate buffers are two fixed
 // slots of the caller's workspace.
+#include <algorithm>
 #include <map>
 #include <tuple>
 
@@ -114,12 +115,55 @@ int sm_count(int device)
     return n;
 }
 
+// Copy of a 1D row plan's steps re-targeted to `rows` (<= the planned
+// batch) transforms, so one resident plan serves batches of any size.
+bool scale_steps_to_rows(const Plan &p, int64_t rows, std::vector<Step> &out)
+{
+    if (p.sizes.size() != 1 || p.vertical || rows <= 0 || rows > p.batch) return false;
+    out = p.steps;
+    for (Step &s : out) {
+        if (s.kind != StepKind::kTile) {
+            s.rows = rows;
+            continue;
+        }
+        TileDesc &d = s.d;
+        if (d.n_outer == 1 && !d.xfast) {
+            d.n_cols = rows;  // batched rows
+            d.tiles_per_outer = (rows + d.tb - 1) / d.tb;
+            d.num_tiles = d.tiles_per_outer;
+        } else if (d.n_outer == p.batch) {
+            d.n_outer = rows;  // multi-pass: one outer group per transform
+            d.num_tiles = d.tiles_per_outer * rows;
+        } else {
+            return false;
+        }
+        s.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(d.num_tiles, s.grid)));
+        if (s.has_row) {
+            TileDesc &r = s.rd;
+            r.n_cols = rows;
+            r.num_tiles = (rows + r.tb - 1) / r.tb;
+            r.tiles_per_outer = r.num_tiles;
+            s.row_grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(r.num_tiles, s.row_grid)));
+        }
+    }
+    return true;
+}
+
+cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const void *in, void *out, void *workspace,
+                          cudaStream_t st);
+
 cudaError_t execute_plan(Plan &p, const void *in, void *out, cudaStream_t st)
 {
-    char *ws = static_cast<char *>(p.workspace);
+    return execute_steps(p, p.steps, in, out, p.workspace, st);
+}
+
+cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const void *in, void *out, void *workspace,
+                          cudaStream_t st)
+{
+    char *ws = static_cast<char *>(workspace);
     const size_t off1 = (p.ws_buf_bytes[0] + 255) / 256 * 256;
     void *bufs[4] = {const_cast<void *>(in), out, ws, ws ? ws + off1 : nullptr};
-    for (const Step &s : p.steps) {
+    for (const Step &s : steps) {
         const void *src = bufs[static_cast<int>(s.src)];
         void *dst = bufs[static_cast<int>(s.dst)];
         if (src == nullptr || dst == nullptr) return cudaErrorInvalidDevicePointer;

@@ -143,6 +143,10 @@ std::string build_plan_2d(Plan &p);
 std::string build_plan_3d(Plan &p);
 // Launch every step of an initialised plan.
 cudaError_t execute_plan(Plan &p, const void *in, void *out, cudaStream_t st);
+// Same for an explicit step list (e.g. re-targeted to fewer rows) and workspace.
+cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const void *in, void *out, void *workspace,
+                          cudaStream_t st);
+bool scale_steps_to_rows(const Plan &p, int64_t rows, std::vector<Step> &out);
 std::string describe_plan(const Plan &p);
 
 // Radix decomposition used by the tile kernel (largest radices first).

@@ -58,6 +58,8 @@ EXPORTED_SYMBOLS = (
     "asdFftExecRaw", "asdFftDescribePlan", "asdFftPlanLaunchCount",
     "asdFftBatchPlanCreate", "asdFftBatchGetWorkspaceSize", "asdFftBatchExec", "asdFftBatchPlanDestroy",
     "asdFftBatchDescribe", "asdFftAutotune", "asdFftTuneCacheLoad",
+    "asdFftServerCreate", "asdFftServerWarm", "asdFftServerSubmit", "asdFftServerDrain", "asdFftServerBatches",
+    "asdFftServerDestroy", "asdFftServeRun",
 )
 
 
@@ -113,6 +115,16 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "asdFftBatchDescribe": (i64, [vp, ctypes.c_char_p, i64]),
         "asdFftAutotune": (i32, [P64, P64, i32, i32, ctypes.c_char_p]),
         "asdFftTuneCacheLoad": (i32, [ctypes.c_char_p]),
+        "asdFftServerCreate": (i32, [ctypes.POINTER(vp), i64, i32, i64, i32]),
+        "asdFftServerWarm": (i32, [vp, i32, i32, i64]),
+        "asdFftServerSubmit": (i64, [vp, i32, i32, i64, i64, vp, vp]),
+        "asdFftServerDrain": (i64, [vp, P64, ctypes.POINTER(ctypes.c_double), i64]),
+        "asdFftServerBatches": (i64, [vp]),
+        "asdFftServerDestroy": (i32, [vp]),
+        "asdFftServeRun": (ctypes.c_double, [vp, ctypes.c_double, i64, ctypes.c_uint64, i32,
+                                             ctypes.POINTER(ctypes.c_int32), P64, ctypes.POINTER(vp),
+                                             ctypes.POINTER(vp), i64, i64, i32, ctypes.POINTER(ctypes.c_double),
+                                             P64, ctypes.POINTER(ctypes.c_int32)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -386,3 +398,64 @@ def autotune(groups, direction=ASCEND_FFT_FORWARD, cache_path: Optional[str] = N
 
 def tune_cache_load(cache_path: str) -> int:
     return load_library().asdFftTuneCacheLoad(cache_path.encode())
+
+
+# --- continuous-batching server --------------------------------------------------------------------
+class Server:
+    """The library's C++ continuous-batching FFT server (see include/asdsip_fft_ext.h)."""
+
+    def __init__(self, budget_bytes=32 << 30, lanes=4, max_rows=1024, device_io=False):
+        h = ctypes.c_void_p()
+        st = load_library().asdFftServerCreate(ctypes.byref(h), int(budget_bytes), int(lanes), int(max_rows),
+                                               1 if device_io else 0)
+        if st != ACL_SUCCESS:
+            raise FftError("asdFftServerCreate", st)
+        self.handle = h.value
+
+    def warm(self, fft_type, direction, n):
+        return load_library().asdFftServerWarm(self.handle, fft_type, direction, n)
+
+    def submit(self, fft_type, direction, n, rows, in_ptr, out_ptr) -> int:
+        return load_library().asdFftServerSubmit(self.handle, fft_type, direction, n, rows, in_ptr, out_ptr)
+
+    def drain(self, cap=1 << 20):
+        import numpy as np
+
+        ids = np.zeros(cap, np.int64)
+        lat = np.zeros(cap, np.float64)
+        n = load_library().asdFftServerDrain(self.handle, ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                             lat.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cap)
+        n = min(n, cap)
+        return ids[:n], lat[:n]
+
+    def batches(self) -> int:
+        return load_library().asdFftServerBatches(self.handle)
+
+    def run_poisson(self, rate, count, seed, classes, pool_in, pool_out, rows_min, rows_max,
+                    direction=ASCEND_FFT_FORWARD):
+        import numpy as np
+
+        k = len(classes)
+        types = (ctypes.c_int32 * k)(*[int(t) for t, _ in classes])
+        sizes = (ctypes.c_int64 * k)(*[int(n) for _, n in classes])
+        pin = (ctypes.c_void_p * k)(*pool_in)
+        pout = (ctypes.c_void_p * k)(*pool_out)
+        lat = np.zeros(count, np.float64)
+        rows = np.zeros(count, np.int64)
+        cls = np.zeros(count, np.int32)
+        wall = load_library().asdFftServeRun(
+            self.handle, float(rate), int(count), int(seed), k, types, sizes, pin, pout, int(rows_min),
+            int(rows_max), direction, lat.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            rows.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), cls.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        return wall, lat, rows, cls
+
+    def close(self):
+        if self.handle:
+            load_library().asdFftServerDestroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
