@@ -54,6 +54,8 @@ struct GlobalRow {
 
 template <int MAXE>
 struct RuntimeEngine {
+    static constexpr int kMaxThreads = 512;
+    static constexpr int kMinBlocks = 1;
     template <bool FWD, class Src0, class DstL>
     __device__ __forceinline__ static void run(const TileDesc &d, float2 *work, const Src0 &src0, const DstL &dstL,
                                                bool dst_in_place, int lane, bool active)
@@ -81,7 +83,8 @@ __device__ __forceinline__ void r2c_post_row(const float2 *work, float2 *y, int 
 }
 
 template <class Engine, bool FWD, int IO>
-__global__ void __launch_bounds__(512, 1) pipelined_rows_kernel(const __grid_constant__ TileDesc d, int *err)
+__global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
+    pipelined_rows_kernel(const __grid_constant__ TileDesc d, int *err)
 {
     extern __shared__ __align__(128) unsigned char smraw[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smraw);

@@ -240,7 +240,9 @@ struct Builder {
                 stw = t->ptr;
                 c.tpt = sk->tpt;
                 c.tb = std::max(1, std::min(kRowThreadsTarget / sk->tpt, static_cast<int>(std::min<int64_t>(rows, 64))));
-                while (c.tb > 1 && c.tb * c.tpt > kMaxThreads) c.tb /= 2;
+                // static engines are built for 256-thread CTAs (512 only when one transform needs them)
+                const int cap = sk->tpt <= 256 ? 256 : kMaxThreads;
+                while (c.tb > 1 && c.tb * c.tpt > cap) c.tb /= 2;
             } else {
                 sk = nullptr;
                 err.clear();

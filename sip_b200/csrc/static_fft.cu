@@ -108,8 +108,14 @@ __device__ __forceinline__ void srun(float2 *v, float2 *work, const Src0 &src0, 
     }
 }
 
+// Up to 256 threads per CTA the engines are compiled for three resident CTAs
+// per SM (at most 85 registers per thread: the codelets fit without
+// spilling), which doubles the warps available to hide shared-memory and
+// twiddle-load latency compared with an unconstrained build.
 template <class Q, int T>
 struct StaticEngine {
+    static constexpr int kMaxThreads = T <= 256 ? 256 : T;
+    static constexpr int kMinBlocks = T <= 256 ? 3 : 1;
     template <bool FWD, class Src0, class DstL>
     __device__ __forceinline__ static void run(const TileDesc &d, float2 *work, const Src0 &src0, const DstL &dstL,
                                                bool dst_in_place, int lane, bool active)
