@@ -22,6 +22,9 @@ ASDSIP_API int32_t asdFftExecRaw(void *handle, const void *input, void *output);
  * (NUL-terminated, truncated to len).  Returns the full length needed. */
 ASDSIP_API int64_t asdFftDescribePlan(void *handle, char *buf, int64_t len);
 
+/* Message of the last failing call on the calling thread (NUL-terminated); returns the length needed. */
+ASDSIP_API int64_t asdFftGetErrorMessage(char *buf, int64_t len);
+
 /* Number of kernel launches one execution of the plan issues. */
 ASDSIP_API int32_t asdFftPlanLaunchCount(void *handle);
 
@@ -58,6 +61,8 @@ ASDSIP_API int64_t asdFftServerSubmit(void *server, int32_t type, int32_t direct
 /* Waits for every submitted request; writes up to cap (id, latency in seconds; < 0 = failed). */
 ASDSIP_API int64_t asdFftServerDrain(void *server, int64_t *ids, double *latency_s, int64_t cap);
 ASDSIP_API int64_t asdFftServerBatches(void *server);
+/* hold != 0: keep admitting nothing (requests queue); 0: resume. */
+ASDSIP_API int32_t asdFftServerHold(void *server, int32_t hold);
 ASDSIP_API int32_t asdFftServerDestroy(void *server);
 /* Poisson load generator over per-class input/output pools; returns wall seconds (< 0 on error). */
 ASDSIP_API double asdFftServeRun(void *server, double rate, int64_t count, uint64_t seed, int32_t nclasses,

@@ -62,6 +62,7 @@ bool log_enabled()
 
 void log_error(const char *where, const std::string &msg)
 {
+    sipfft::set_last_error(std::string(where) + ": " + msg);
     if (log_enabled()) std::fprintf(stderr, "[asdsip_fft] %s: %s\n", where, msg.c_str());
 }
 
@@ -484,6 +485,17 @@ int64_t asdFftDescribePlan(void *handle, char *buf, int64_t len)
         std::lock_guard<std::mutex> lock(p->mu);
         s = sipfft::describe_plan(*p);
     }
+    if (buf && len > 0) {
+        const int64_t n = std::min<int64_t>(len - 1, static_cast<int64_t>(s.size()));
+        std::memcpy(buf, s.data(), static_cast<size_t>(n));
+        buf[n] = '\0';
+    }
+    return static_cast<int64_t>(s.size()) + 1;
+}
+
+int64_t asdFftGetErrorMessage(char *buf, int64_t len)
+{
+    const std::string &s = sipfft::last_error();
     if (buf && len > 0) {
         const int64_t n = std::min<int64_t>(len - 1, static_cast<int64_t>(s.size()));
         std::memcpy(buf, s.data(), static_cast<size_t>(n));

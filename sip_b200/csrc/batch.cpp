@@ -429,6 +429,7 @@ int32_t asdFftBatchPlanCreate(void **plan, const int64_t *sizes, const int64_t *
         if (tune_cache && *tune_cache) sipfft::load_tune_cache(tune_cache, bp->device);
         std::string e = sipfft::build_batch(*bp);
         if (!e.empty()) {
+            sipfft::set_last_error("asdFftBatchPlanCreate: " + e);
             if (std::getenv("ASDSIP_FFT_LOG")) std::fprintf(stderr, "[asdsip_fft] batch plan: %s\n", e.c_str());
             return e.rfind("twiddle table", 0) == 0 ? AsdSip::ACL_ERROR_INTERNAL_ERROR
                                                     : AsdSip::ACL_ERROR_API_NOT_SUPPORT;

@@ -493,7 +493,7 @@ cudaError_t launch_batch(int grid, int block, size_t smem, const BatchSeg *segs,
     const void *fn = batch_kernel_fn();
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBytes);
+        cudaError_t e = allow_max_dynamic_smem(fn);
         if (e != cudaSuccess) return e;
         configured = true;
     }

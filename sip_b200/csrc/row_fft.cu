@@ -34,11 +34,22 @@ const void *pick(const TileDesc &d, int maxe, bool forward)
 
 size_t row_kernel_smem(const TileDesc &d) { return 128 + 2 * static_cast<size_t>(d.g_ns) * sizeof(float2); }
 
+// Raises a kernel's dynamic shared-memory limit to what the SM allows next
+// to the kernel's static shared memory.
+cudaError_t allow_max_dynamic_smem(const void *fn)
+{
+    cudaFuncAttributes attr{};
+    cudaError_t e = cudaFuncGetAttributes(&attr, fn);
+    if (e != cudaSuccess) return e;
+    const int limit = kMaxSmemBytes - static_cast<int>(attr.sharedSizeBytes);
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+}
+
 int kernel_blocks_per_sm(const void *fn, int threads, size_t smem)
 {
     int nb = 0;
     if (!fn) return 0;
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBytes) != cudaSuccess ||
+    if (allow_max_dynamic_smem(fn) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -67,8 +78,7 @@ cudaError_t launch_row_tiles(const TileDesc &d, int maxe, bool forward, int grid
     const int mi = maxe <= 8 ? 0 : (maxe <= 16 ? 1 : 2);
     const int ii = d.io == IO_C2C ? 0 : (d.io == IO_R2C_PACKED ? 1 : 2);
     if (!configured[mi][forward][ii]) {
-        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBytes) != cudaSuccess)
-            return cudaGetLastError();
+        if (allow_max_dynamic_smem(fn) != cudaSuccess) return cudaGetLastError();
         configured[mi][forward][ii] = true;
     }
     return launch_kernel_fn(fn, d, grid, row_kernel_smem(d), err, st);

@@ -81,6 +81,13 @@ TablePtr get_stage_table(const StaticKernel &k, int device, std::string *err)
 }
 
 namespace {
+thread_local std::string t_last_error;
+}  // namespace
+
+void set_last_error(const std::string &msg) { t_last_error = msg; }
+const std::string &last_error() { return t_last_error; }
+
+namespace {
 std::mutex g_dev_mu;
 std::map<int, int *> g_err_words;
 std::map<int, int> g_sms;

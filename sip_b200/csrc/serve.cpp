@@ -100,11 +100,39 @@ public:
         cudaGetLastError();
     }
 
-    // Creates the resident plan of a request class ahead of traffic.
+    // Creates the resident plan of a request class ahead of traffic and
+    // grows every lane's staging buffers to that class's largest batch, so no
+    // allocation happens while requests are timed.
     std::string warm(int type, int dir, int64_t n)
     {
-        std::lock_guard<std::mutex> lock(plan_mu_);
-        return plan_for(type, dir, n) ? std::string() : last_err_;
+        Plan *p = nullptr;
+        {
+            std::lock_guard<std::mutex> lock(plan_mu_);
+            p = plan_for(type, dir, n);
+            if (!p) return last_err_;
+        }
+        Req probe;
+        probe.type = type;
+        probe.n = n;
+        probe.rows = max_rows_;
+        std::lock_guard<std::mutex> lock(lane_mu_);
+        for (Lane &l : lanes_) {
+            if (l.busy) continue;
+            if (!grow(l.d_in, l.bytes_in, static_cast<size_t>(in_bytes(probe))) ||
+                !grow(l.d_out, l.bytes_out, static_cast<size_t>(out_bytes(probe))) ||
+                !grow(l.d_ws, l.bytes_ws, std::max<size_t>(p->ws_bytes, 256)))
+                return "out of device memory";
+        }
+        return std::string();
+    }
+
+    // While held, pending requests are queued but not admitted (operators can
+    // drain lanes; tests use it to make batching deterministic).
+    void hold(bool on)
+    {
+        std::lock_guard<std::mutex> lock(mu_);
+        hold_ = on;
+        cv_.notify_all();
     }
 
     int64_t submit(Req r)
@@ -188,7 +216,7 @@ private:
     // requests as fit the lane and the budget (caller holds mu_).
     bool form_batch(std::vector<Req> &batch, int64_t &bytes)
     {
-        if (pending_.empty()) return false;
+        if (pending_.empty() || hold_) return false;
         const Req head = pending_.front();
         int64_t rows = 0;
         bytes = 0;
@@ -256,6 +284,8 @@ private:
             }
             // admissions
             bool launched = false;
+            {
+            std::lock_guard<std::mutex> lanes_lock(lane_mu_);
             for (Lane &l : lanes_) {
                 if (l.busy) continue;
                 std::vector<Req> batch;
@@ -277,6 +307,7 @@ private:
                     finish_lane(l, -1.0);  // reported with a negative completion time
                 }
                 launched = true;
+            }
             }
             {
                 std::unique_lock<std::mutex> lock(mu_);
@@ -313,6 +344,8 @@ private:
     int64_t inflight_ = 0;
     int64_t next_id_ = 0;
     bool stop_ = false;
+    bool hold_ = false;
+    std::mutex lane_mu_;
     std::atomic<int64_t> batches_{0}, failures_{0};
     std::thread worker_;
 };
@@ -394,6 +427,14 @@ int64_t asdFftServerDrain(void *server, int64_t *ids, double *latency_s, int64_t
         if (latency_s) latency_s[i] = done[i].t_done < 0 ? -1.0 : done[i].t_done - done[i].t_submit;
     }
     return static_cast<int64_t>(done.size());
+}
+
+int32_t asdFftServerHold(void *server, int32_t hold)
+{
+    sipfft::Server *s = find_server(server);
+    if (!s) return AsdSip::ACL_ERROR_INVALID_PARAM;
+    s->hold(hold != 0);
+    return AsdSip::ACL_SUCCESS;
 }
 
 int64_t asdFftServerBatches(void *server)

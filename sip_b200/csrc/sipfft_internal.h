@@ -30,6 +30,7 @@ cudaError_t launch_row_tiles(const TileDesc &d, int maxe, bool forward, int grid
 size_t row_kernel_smem(const TileDesc &d);
 int row_kernel_blocks_per_sm(const TileDesc &d, int maxe, bool forward);
 int kernel_blocks_per_sm(const void *fn, int threads, size_t smem);
+cudaError_t allow_max_dynamic_smem(const void *fn);
 // persistent uneven-batch kernel (fft_tile.cu)
 const void *batch_kernel_fn();
 cudaError_t launch_batch(int grid, int block, size_t smem, const BatchSeg *segs, const int2 *items, int nitems,
@@ -50,6 +51,9 @@ int64_t stage_twiddle_count(const int *radix, int nstages);
 // Process-wide device error word of the current device (bounded waits that
 // gave up set it); read and cleared by asdFftSynchronize.
 int *device_error_word(int device);
+// Message of the last failing call on this thread (asdFftGetErrorMessage).
+void set_last_error(const std::string &msg);
+const std::string &last_error();
 int sm_count(int device);
 // R2C post-twiddle / C2R pre-twiddle of the multi-pass (large-N) plans.
 cudaError_t launch_r2c_post(const float2 *z, float2 *x, int64_t rows, int64_t m, int64_t zdist, int64_t xdist,

@@ -59,14 +59,27 @@ EXPORTED_SYMBOLS = (
     "asdFftBatchPlanCreate", "asdFftBatchGetWorkspaceSize", "asdFftBatchExec", "asdFftBatchPlanDestroy",
     "asdFftBatchDescribe", "asdFftAutotune", "asdFftTuneCacheLoad",
     "asdFftServerCreate", "asdFftServerWarm", "asdFftServerSubmit", "asdFftServerDrain", "asdFftServerBatches",
-    "asdFftServerDestroy", "asdFftServeRun",
+    "asdFftServerDestroy", "asdFftServeRun", "asdFftServerHold", "asdFftGetErrorMessage",
 )
 
 
 class FftError(RuntimeError):
     def __init__(self, where: str, status: int):
-        super().__init__(f"{where} returned {status}")
+        msg = ""
+        try:
+            msg = last_error_message()
+        except Exception:
+            pass
+        super().__init__(f"{where} returned {status}" + (f" ({msg})" if msg else ""))
         self.status = status
+
+
+def last_error_message() -> str:
+    lib = load_library()
+    n = lib.asdFftGetErrorMessage(None, 0)
+    buf = ctypes.create_string_buffer(int(max(1, n)))
+    lib.asdFftGetErrorMessage(buf, n)
+    return buf.value.decode(errors="replace")
 
 
 _lib: Optional[ctypes.CDLL] = None
@@ -120,6 +133,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "asdFftServerSubmit": (i64, [vp, i32, i32, i64, i64, vp, vp]),
         "asdFftServerDrain": (i64, [vp, P64, ctypes.POINTER(ctypes.c_double), i64]),
         "asdFftServerBatches": (i64, [vp]),
+        "asdFftServerHold": (i32, [vp, i32]),
+        "asdFftGetErrorMessage": (i64, [ctypes.c_char_p, i64]),
         "asdFftServerDestroy": (i32, [vp]),
         "asdFftServeRun": (ctypes.c_double, [vp, ctypes.c_double, i64, ctypes.c_uint64, i32,
                                              ctypes.POINTER(ctypes.c_int32), P64, ctypes.POINTER(vp),
@@ -430,6 +445,9 @@ class Server:
 
     def batches(self) -> int:
         return load_library().asdFftServerBatches(self.handle)
+
+    def hold(self, on: bool = True):
+        return load_library().asdFftServerHold(self.handle, 1 if on else 0)
 
     def run_poisson(self, rate, count, seed, classes, pool_in, pool_out, rows_min, rows_max,
                     direction=ASCEND_FFT_FORWARD):
