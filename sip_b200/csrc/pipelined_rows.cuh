@@ -52,18 +52,6 @@ struct GlobalRow {
     __device__ __forceinline__ void operator()(int e, float2 v) const { row[e] = v; }
 };
 
-template <int MAXE>
-struct RuntimeEngine {
-    static constexpr int kMaxThreads = 512;
-    static constexpr int kMinBlocks = 1;
-    template <bool FWD, class Src0, class DstL>
-    __device__ __forceinline__ static void run(const TileDesc &d, float2 *work, const Src0 &src0, const DstL &dstL,
-                                               bool dst_in_place, int lane, bool active)
-    {
-        run_fft<MAXE, FWD>(d, work, src0, true, dstL, dst_in_place, lane, active);
-    }
-};
-
 // R2C post-twiddle from the padded work row to HBM: X[k] = E + w^k O,
 // X[n-k] = conj(E - w^k O) with E, O recovered from Z[k], conj(Z[n-k]).
 template <bool FWD>
@@ -81,6 +69,27 @@ __device__ __forceinline__ void r2c_post_row(const float2 *work, float2 *y, int 
         if (2 * k != n) y[n - k] = cconj(csub(e, wo));
     }
 }
+
+template <int MAXE>
+struct RuntimeEngine {
+    static constexpr int kMaxThreads = 512;
+    static constexpr int kMinBlocks = 1;
+    template <bool FWD, class Src0, class DstL>
+    __device__ __forceinline__ static void run(const TileDesc &d, float2 *work, const Src0 &src0, const DstL &dstL,
+                                               bool dst_in_place, int lane, bool active)
+    {
+        run_fft<MAXE, FWD>(d, work, src0, true, dstL, dst_in_place, lane, active);
+    }
+    // R2C: packed FFT into the work row, then the post-twiddle pass to HBM
+    template <bool FWD, class Src0>
+    __device__ __forceinline__ static void run_r2c(const TileDesc &d, float2 *work, const Src0 &src0, float2 *y,
+                                                   int lane, bool active)
+    {
+        run_fft<MAXE, FWD>(d, work, src0, true, SmemRow{work}, true, lane, active);
+        __syncthreads();
+        if (active) r2c_post_row<FWD>(work, y, d.n, lane, d.tpt, d.tw);
+    }
+};
 
 template <class Engine, bool FWD, int IO>
 __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
@@ -148,10 +157,9 @@ __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
         } else if constexpr (IO == IO_C2R_PACKED) {
             Engine::template run<FWD>(d, work, C2RPre<FWD>{buf + l * in_dist, d.n, d.tw},
                                       GlobalRow{out + row_index * out_dist}, false, lane, active);
-        } else {  // IO_R2C_PACKED: FFT into the work rows, then the post-twiddle to HBM
-            Engine::template run<FWD>(d, work, StageRow{buf + l * in_dist}, SmemRow{work}, true, lane, active);
-            __syncthreads();
-            if (active) r2c_post_row<FWD>(work, out + row_index * out_dist, d.n, lane, tpt, d.tw);
+        } else {  // IO_R2C_PACKED
+            Engine::template run_r2c<FWD>(d, work, StageRow{buf + l * in_dist}, out + row_index * out_dist, lane,
+                                          active);
         }
         __syncthreads();  // buffer b is free for the copy issued in iteration i+1
     }

@@ -231,7 +231,7 @@ struct Builder {
     {
         const int64_t rows = s.d.n_cols;
         TileCfg c = c0;
-        const StaticKernel *sk = find_static_kernel(s.d.n);
+        const StaticKernel *sk = find_static_kernel(s.d.n, s.d.io);
         const float2 *stw = nullptr;
         if (sk) {
             TablePtr t = get_stage_table(*sk, device, &err);

@@ -58,9 +58,11 @@ TablePtr get_table(int64_t count, int64_t denom, int64_t mult, int device, std::
 TablePtr get_stage_table(const StaticKernel &k, int device, std::string *err)
 {
     static std::mutex mu;
-    static std::map<std::pair<int, int>, std::weak_ptr<DeviceTable>> cache;  // (device, n)
+    static std::map<std::pair<int, std::string>, std::weak_ptr<DeviceTable>> cache;  // (device, radix sequence)
     std::lock_guard<std::mutex> lock(mu);
-    auto key = std::make_pair(device, k.n);
+    std::string seq;
+    for (int s = 0; s < k.nstages; s++) seq += std::to_string(k.radix[s]) + ",";
+    auto key = std::make_pair(device, seq);
     auto it = cache.find(key);
     if (it != cache.end()) {
         if (TablePtr t = it->second.lock()) return t;

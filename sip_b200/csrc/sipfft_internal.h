@@ -39,13 +39,14 @@ cudaError_t launch_kernel_fn(const void *fn, const TileDesc &d, int grid, size_t
 
 // Compile-time specialised pipelined row kernels (static_fft.cu).
 struct StaticKernel {
+    int io_mask = 7;  // bit 0: C2C, bit 1: C2R (packed), bit 2: R2C (packed)
     int n = 0;
     int nstages = 0;
     int radix[8] = {};
     int tpt = 0;
     const void *fn[2][3] = {};  // [forward][C2C, R2C packed, C2R packed]
 };
-const StaticKernel *find_static_kernel(int n);
+const StaticKernel *find_static_kernel(int n, int io);
 cudaError_t fill_stage_twiddles(float2 *t, const int *radix, int nstages, cudaStream_t st);
 int64_t stage_twiddle_count(const int *radix, int nstages);
 // Process-wide device error word of the current device (bounded waits that

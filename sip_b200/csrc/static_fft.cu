@@ -112,6 +112,67 @@ __device__ __forceinline__ void srun(float2 *v, float2 *work, const Src0 &src0, 
 // per SM (at most 85 registers per thread: the codelets fit without
 // spilling), which doubles the warps available to hide shared-memory and
 // twiddle-load latency compared with an unconstrained build.
+// R2C post-twiddle value for bin k from Z[k] and conj(Z[m-k]):
+// X[k] = E + w^k O, E = (Z[k] + conj Z[m-k]) / 2, O = -i (Z[k] - conj Z[m-k]) / 2.
+template <bool FWD>
+__device__ __forceinline__ float2 r2c_bin(float2 zk, float2 zmc, float2 w, float2 &e, float2 &wo)
+{
+    e = cscale(cadd(zk, zmc), 0.5f);
+    const float2 t = csub(zk, zmc);
+    wo = cmul(w, make_float2(0.5f * t.y, -0.5f * t.x));
+    return cadd(e, wo);
+}
+
+// Last stage of an R2C transform with the post-twiddle fused: the thread owns
+// butterflies j0 = lane and its mirror j1 = NBF - lane (lane 0: j1 = NBF/2),
+// so the partner Z[m-k] of every output k it produces is in its own
+// registers, and the N/2+1 bins are written straight to HBM.
+template <class Q, int T, bool FWD>
+struct FusedR2C {
+    static constexpr int S = Q::S - 1;
+    static constexpr int R = Q::r[S], N = Q::N, NS = Q::ns(S), NBF = N / R;
+    static constexpr bool ok = Q::S >= 2 && NBF % 2 == 0 && T == NBF / 2;
+
+    __device__ __forceinline__ static void run(float2 *v, const float2 *work, float2 *y, int lane, bool active,
+                                               const float2 *__restrict__ stw, const float2 *__restrict__ tw)
+    {
+        const int j0 = lane, j1 = lane == 0 ? NBF / 2 : NBF - lane;
+        if (active) {
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                v[r] = work[pad(j0 + r * NBF)];
+                v[R + r] = work[pad(j1 + r * NBF)];
+            }
+            const float2 *t0 = stw + Q::tw_off(S) + j0;
+            const float2 *t1 = stw + Q::tw_off(S) + j1;
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                v[r] = cmul(v[r], dir<FWD>(__ldg(t0 + (r - 1) * NS)));
+                v[R + r] = cmul(v[R + r], dir<FWD>(__ldg(t1 + (r - 1) * NS)));
+            }
+            dft<R, FWD>(v);
+            dft<R, FWD>(v + R);
+            float2 e, wo;
+            if (lane != 0) {
+#pragma unroll
+                for (int r = 0; r < R; r++) {
+                    const int k0 = j0 + r * NBF, k1 = j1 + r * NBF;
+                    y[k0] = r2c_bin<FWD>(v[r], cconj(v[R + R - 1 - r]), dir<FWD>(__ldg(tw + k0)), e, wo);
+                    y[k1] = r2c_bin<FWD>(v[R + r], cconj(v[R - 1 - r]), dir<FWD>(__ldg(tw + k1)), e, wo);
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; r++) {
+                    const int k0 = r * NBF, k1 = NBF / 2 + r * NBF;
+                    y[k0] = r2c_bin<FWD>(v[r], cconj(v[(R - r) % R]), dir<FWD>(__ldg(tw + k0)), e, wo);
+                    if (r == 0) y[N] = cconj(csub(e, wo));  // Nyquist bin from the k = 0 pair
+                    y[k1] = r2c_bin<FWD>(v[R + r], cconj(v[R + R - 1 - r]), dir<FWD>(__ldg(tw + k1)), e, wo);
+                }
+            }
+        }
+    }
+};
+
 template <class Q, int T>
 struct StaticEngine {
     static constexpr int kMaxThreads = T <= 256 ? 256 : T;
@@ -123,15 +184,58 @@ struct StaticEngine {
         float2 v[static_maxv<Q, T>()];
         srun<Q, T, FWD, 0>(v, work, src0, dstL, dst_in_place, lane, active, d.stw);
     }
+
+    template <bool FWD, class Src0>
+    __device__ __forceinline__ static void run_r2c(const TileDesc &d, float2 *work, const Src0 &src0, float2 *y,
+                                                   int lane, bool active)
+    {
+        using F = FusedR2C<Q, T, FWD>;
+        if constexpr (F::ok) {
+            constexpr int V = static_maxv<Q, T>() > 2 * F::R ? static_maxv<Q, T>() : 2 * F::R;
+            float2 v[V];
+            srun_prefix<FWD>(v, work, src0, lane, active, d.stw);
+            __syncthreads();
+            F::run(v, work, y, lane, active, d.stw, d.tw);
+        } else {
+            run<FWD>(d, work, src0, SmemRow{work}, true, lane, active);
+            __syncthreads();
+            if (active) r2c_post_row<FWD>(work, y, d.n, lane, d.tpt, d.tw);
+        }
+    }
+
+    // every stage but the last, leaving the data in the padded work row
+    template <bool FWD, class Src0>
+    __device__ __forceinline__ static void srun_prefix(float2 *v, float2 *work, const Src0 &src0, int lane,
+                                                       bool active, const float2 *stw)
+    {
+        prefix<FWD, 0>(v, work, src0, lane, active, stw);
+    }
+    template <bool FWD, int S, class Src0>
+    __device__ __forceinline__ static void prefix(float2 *v, float2 *work, const Src0 &src0, int lane, bool active,
+                                                  const float2 *stw)
+    {
+        if constexpr (S < Q::S - 1) {
+            const SmemRow w{work};
+            if constexpr (S == 0)
+                sgather<Q, 0, T, FWD>(v, src0, lane, active, stw);
+            else
+                sgather<Q, S, T, FWD>(v, w, lane, active, stw);
+            __syncthreads();
+            sscatter<Q, S, T>(v, w, lane, active);
+            if constexpr (S + 1 < Q::S - 1) __syncthreads();
+            prefix<FWD, S + 1>(v, work, src0, lane, active, stw);
+        }
+    }
 };
 
 // ------------------------------------------------------------------------------------ registry
 namespace {
 
 template <class Q, int T>
-StaticKernel make_entry()
+StaticKernel make_entry(int io_mask = 7)
 {
     StaticKernel e{};
+    e.io_mask = io_mask;
     e.n = Q::N;
     e.nstages = Q::S;
     for (int s = 0; s < Q::S; s++) e.radix[s] = Q::r[s];
@@ -157,17 +261,19 @@ const std::vector<StaticKernel> &registry()
         make_entry<Seq<16, 16, 8>, 128>(),      // 2048
         make_entry<Seq<16, 16, 16>, 256>(),     // 4096
         make_entry<Seq<16, 16, 16, 2>, 512>(),  // 8192
-        make_entry<Seq<10, 10, 15>, 100>(),     // 1500 (packed half of the 3000-point real transform)
+        make_entry<Seq<10, 10, 15>, 100>(3),    // 1500: C2C, and C2R of the 3000-point real transform
+        make_entry<Seq<10, 15, 10>, 75>(2),     // 1500: R2C of 3000 with the fused post-twiddle (T = NBF/2)
     };
     return r;
 }
 
 }  // namespace
 
-const StaticKernel *find_static_kernel(int n)
+const StaticKernel *find_static_kernel(int n, int io)
 {
+    const int bit = io == IO_C2C ? 1 : (io == IO_C2R_PACKED ? 2 : (io == IO_R2C_PACKED ? 4 : 0));
     for (const StaticKernel &e : registry())
-        if (e.n == n) return &e;
+        if (e.n == n && (e.io_mask & bit)) return &e;
     return nullptr;
 }
 
