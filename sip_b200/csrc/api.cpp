@@ -107,6 +107,12 @@ AspbStatus finish_plan(sipfft::Plan &p, std::string (*builder)(sipfft::Plan &), 
         return ACL_ERROR_INTERNAL_ERROR;
     }
     p.device = dev;
+    if (sipfft::configure_kernels(dev) != cudaSuccess) {
+        cudaGetLastError();
+        p.failed = true;
+        log_error(where, "kernel configuration failed");
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
     std::string err;
     try {
         err = builder(p);

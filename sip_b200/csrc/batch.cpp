@@ -416,7 +416,7 @@ int32_t asdFftBatchPlanCreate(void **plan, const int64_t *sizes, const int64_t *
         return AsdSip::ACL_ERROR_INVALID_PARAM;
     try {
         auto bp = std::make_unique<BatchPlan>();
-        if (cudaGetDevice(&bp->device) != cudaSuccess) {
+        if (cudaGetDevice(&bp->device) != cudaSuccess || sipfft::configure_kernels(bp->device) != cudaSuccess) {
             cudaGetLastError();
             return AsdSip::ACL_ERROR_INTERNAL_ERROR;
         }
@@ -489,6 +489,7 @@ int32_t asdFftBatchExec(void *plan, const void *input, void *output, void *works
             if (e == cudaSuccess) e = cudaGraphInstantiate(&bp->gexec, bp->graph, 0);
             if (own) cudaStreamDestroy(cap);
             if (e != cudaSuccess) {
+                sipfft::set_last_error(std::string("asdFftBatchExec: graph capture: ") + cudaGetErrorString(e));
                 cudaGetLastError();
                 return AsdSip::ACL_ERROR_INTERNAL_ERROR;
             }
@@ -500,6 +501,7 @@ int32_t asdFftBatchExec(void *plan, const void *input, void *output, void *works
         e = cudaGraphLaunch(bp->gexec, st);
     }
     if (e != cudaSuccess) {
+        sipfft::set_last_error(std::string("asdFftBatchExec: ") + cudaGetErrorString(e));
         cudaGetLastError();
         return AsdSip::ACL_ERROR_INTERNAL_ERROR;
     }
@@ -549,7 +551,7 @@ int32_t asdFftAutotune(const int64_t *sizes, const int64_t *rows, int32_t n, int
 {
     if (!sizes || !rows || n <= 0) return AsdSip::ACL_ERROR_INVALID_PARAM;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
+    if (cudaGetDevice(&dev) != cudaSuccess || sipfft::configure_kernels(dev) != cudaSuccess) {
         cudaGetLastError();
         return AsdSip::ACL_ERROR_INTERNAL_ERROR;
     }

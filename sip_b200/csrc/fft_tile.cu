@@ -16,6 +16,7 @@
 // scatter of the early stages and the column-tile loads are bank-conflict
 // free for 8-byte elements.
 #include <algorithm>
+#include <vector>
 
 #include "codelets.cuh"
 #include "fft_tile.cuh"
@@ -460,17 +461,23 @@ namespace {
 template <int MAXE, bool FWD>
 cudaError_t launch_one(const TileDesc &d, int grid, int block, size_t smem, cudaStream_t st)
 {
-    static bool configured = false;  // attribute is per function; setting it twice is harmless
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(tile_fft_kernel<MAXE, FWD>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBytes);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
     tile_fft_kernel<MAXE, FWD><<<grid, block, smem, st>>>(d);
     return cudaGetLastError();
 }
 }  // namespace
+
+// Kernels of this file whose dynamic shared-memory limit must be raised
+// before their first launch (configure_kernels() in runtime.cpp).
+void tile_kernel_fns(std::vector<const void *> &out)
+{
+    out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<8, true>));
+    out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<8, false>));
+    out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<16, true>));
+    out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<16, false>));
+    out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<32, true>));
+    out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<32, false>));
+    out.push_back(reinterpret_cast<const void *>(batch_fft_kernel<32>));
+}
 
 cudaError_t launch_tile(const TileDesc &d, int maxe, bool forward, int grid, cudaStream_t st)
 {
@@ -491,12 +498,6 @@ cudaError_t launch_batch(int grid, int block, size_t smem, const BatchSeg *segs,
                          int *counter, int *done, const BatchBufs &bufs, int *err, cudaStream_t st)
 {
     const void *fn = batch_kernel_fn();
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = allow_max_dynamic_smem(fn);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
     BatchBufs b = bufs;
     void *args[] = {&segs, &items, &nitems, &counter, &done, &b, &err};
     return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, smem, st);

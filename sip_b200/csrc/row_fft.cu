@@ -1,5 +1,7 @@
 // Runtime-radix instantiation of the TMA-pipelined row kernel
 // (pipelined_rows.cuh) and its host-side launch helpers.
+#include <vector>
+
 #include "pipelined_rows.cuh"
 
 namespace sipfft {
@@ -66,6 +68,18 @@ cudaError_t launch_kernel_fn(const void *fn, const TileDesc &d, int grid, size_t
     return cudaLaunchKernel(fn, dim3(grid), dim3(d.tb * d.tpt), args, smem, st);
 }
 
+void row_kernel_fns(std::vector<const void *> &out)
+{
+    for (int io : {IO_C2C, IO_R2C_PACKED, IO_C2R_PACKED}) {
+        out.push_back(row_fn_io<8, true>(io));
+        out.push_back(row_fn_io<8, false>(io));
+        out.push_back(row_fn_io<16, true>(io));
+        out.push_back(row_fn_io<16, false>(io));
+        out.push_back(row_fn_io<32, true>(io));
+        out.push_back(row_fn_io<32, false>(io));
+    }
+}
+
 int row_kernel_blocks_per_sm(const TileDesc &d, int maxe, bool forward)
 {
     return kernel_blocks_per_sm(pick(d, maxe, forward), d.tb * d.tpt, row_kernel_smem(d));
@@ -73,15 +87,7 @@ int row_kernel_blocks_per_sm(const TileDesc &d, int maxe, bool forward)
 
 cudaError_t launch_row_tiles(const TileDesc &d, int maxe, bool forward, int grid, int *err, cudaStream_t st)
 {
-    const void *fn = pick(d, maxe, forward);
-    static bool configured[3][2][3] = {};
-    const int mi = maxe <= 8 ? 0 : (maxe <= 16 ? 1 : 2);
-    const int ii = d.io == IO_C2C ? 0 : (d.io == IO_R2C_PACKED ? 1 : 2);
-    if (!configured[mi][forward][ii]) {
-        if (allow_max_dynamic_smem(fn) != cudaSuccess) return cudaGetLastError();
-        configured[mi][forward][ii] = true;
-    }
-    return launch_kernel_fn(fn, d, grid, row_kernel_smem(d), err, st);
+    return launch_kernel_fn(pick(d, maxe, forward), d, grid, row_kernel_smem(d), err, st);
 }
 
 }  // namespace sipfft

@@ -110,6 +110,24 @@ int *device_error_word(int device)
     return w;
 }
 
+cudaError_t configure_kernels(int device)
+{
+    static std::mutex mu;
+    static std::map<int, bool> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[device]) return cudaSuccess;
+    std::vector<const void *> fns;
+    tile_kernel_fns(fns);
+    row_kernel_fns(fns);
+    static_kernel_fns(fns);
+    for (const void *fn : fns) {
+        cudaError_t e = allow_max_dynamic_smem(fn);
+        if (e != cudaSuccess) return e;
+    }
+    done[device] = true;
+    return cudaSuccess;
+}
+
 int sm_count(int device)
 {
     std::lock_guard<std::mutex> lock(g_dev_mu);

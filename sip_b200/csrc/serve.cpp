@@ -376,7 +376,7 @@ int32_t asdFftServerCreate(void **server, int64_t budget_bytes, int32_t lanes, i
 {
     if (!server || budget_bytes <= 0 || lanes <= 0 || lanes > 64 || max_rows <= 0) return AsdSip::ACL_ERROR_INVALID_PARAM;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
+    if (cudaGetDevice(&dev) != cudaSuccess || sipfft::configure_kernels(dev) != cudaSuccess) {
         cudaGetLastError();
         return AsdSip::ACL_ERROR_INTERNAL_ERROR;
     }

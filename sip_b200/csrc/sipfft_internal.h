@@ -31,6 +31,14 @@ size_t row_kernel_smem(const TileDesc &d);
 int row_kernel_blocks_per_sm(const TileDesc &d, int maxe, bool forward);
 int kernel_blocks_per_sm(const void *fn, int threads, size_t smem);
 cudaError_t allow_max_dynamic_smem(const void *fn);
+// Raises the dynamic shared-memory limit of every kernel of the library on
+// `device` (once).  Called by every set-up entry point (plan creation, batch
+// plans, servers, the first allocation-free call) so that nothing is
+// configured lazily inside a stream capture.
+cudaError_t configure_kernels(int device);
+void tile_kernel_fns(std::vector<const void *> &out);
+void row_kernel_fns(std::vector<const void *> &out);
+void static_kernel_fns(std::vector<const void *> &out);
 // persistent uneven-batch kernel (fft_tile.cu)
 const void *batch_kernel_fn();
 cudaError_t launch_batch(int grid, int block, size_t smem, const BatchSeg *segs, const int2 *items, int nitems,

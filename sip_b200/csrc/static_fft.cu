@@ -261,13 +261,19 @@ const std::vector<StaticKernel> &registry()
         make_entry<Seq<16, 16, 8>, 128>(),      // 2048
         make_entry<Seq<16, 16, 16>, 256>(),     // 4096
         make_entry<Seq<16, 16, 16, 2>, 512>(),  // 8192
-        make_entry<Seq<10, 10, 15>, 100>(3),    // 1500: C2C, and C2R of the 3000-point real transform
-        make_entry<Seq<10, 15, 10>, 75>(2),     // 1500: R2C of 3000 with the fused post-twiddle (T = NBF/2)
+        make_entry<Seq<10, 10, 15>, 100>(),     // 1500 (packed half of the 3000-point real transform)
     };
     return r;
 }
 
 }  // namespace
+
+void static_kernel_fns(std::vector<const void *> &out)
+{
+    for (const StaticKernel &e : registry())
+        for (int f = 0; f < 2; f++)
+            for (int io = 0; io < 3; io++) out.push_back(e.fn[f][io]);
+}
 
 const StaticKernel *find_static_kernel(int n, int io)
 {
