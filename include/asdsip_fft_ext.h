@@ -70,6 +70,19 @@ ASDSIP_API double asdFftServeRun(void *server, double rate, int64_t count, uint6
                                  void *const *pool_out, int64_t rows_min, int64_t rows_max, int32_t direction,
                                  double *latency_s, int64_t *rows_out, int32_t *class_out);
 
+/* ---- 1D C2C that allocates nothing.  No counterpart in the reference.
+ * For callers that cannot allocate device memory when they need the transform (allocation-free
+ * real-time loops, hosts that own every allocation): the long-transform path normally needs a plan
+ * (cudaMalloc'd twiddle tables) and a caller workspace; this entry point keeps both in a fixed 8.5 MiB
+ * __device__ array of the library instead, held on every GPU that loads the library until exit.
+ * Limits: fftSize in 16385..2^20 splitting into two passes of <= 2048 points (radices 2-16/3/5/7/11/13),
+ * fftSize * batchSize <= 2^20 complex values; larger sizes return ACL_ERROR_INVALID_PARAM.  Same layout
+ * and semantics as a HORIZONTAL C2C plan ([batch, N] complex64, unnormalised, in == out allowed).
+ * Calls that overlap on the GPU share the array and race.  The first call on a device looks up the
+ * array's address; make it before any stream capture. */
+ASDSIP_API int32_t asdFftExecC2CNoAlloc(const void *input, void *output, int64_t fftSize, int64_t batchSize,
+                                        int32_t direction, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

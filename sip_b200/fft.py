@@ -60,6 +60,7 @@ EXPORTED_SYMBOLS = (
     "asdFftBatchDescribe", "asdFftAutotune", "asdFftTuneCacheLoad",
     "asdFftServerCreate", "asdFftServerWarm", "asdFftServerSubmit", "asdFftServerDrain", "asdFftServerBatches",
     "asdFftServerDestroy", "asdFftServeRun", "asdFftServerHold", "asdFftGetErrorMessage",
+    "asdFftExecC2CNoAlloc",
 )
 
 
