@@ -508,6 +508,72 @@ def run_serving(args, world, rank, local):
             "points": points}), flush=True)
 
 
+# ----------------------------------------------------------------------------------- one plan
+def run_kernel(args, world, rank, local):
+    """Times one plan (kind, sizes, batch, direction) on device-resident data: the
+    small-case driver of the profiles and the per-config measurements (the
+    N=1024 C2C case, the 2D / 3D multi-axis transforms)."""
+    import torch
+
+    from sip_b200 import fft
+
+    torch.cuda.set_device(local)
+    kind = {"c2c": fft.ASCEND_FFT_C2C, "r2c": fft.ASCEND_FFT_R2C, "c2r": fft.ASCEND_FFT_C2R}[args.kind]
+    direction = fft.ASCEND_FFT_INVERSE if args.inverse else fft.ASCEND_FFT_FORWARD
+    sizes = [int(v) for v in args.sizes.split(",")]
+    b = args.batch
+    n_total = int(np.prod(sizes))
+    last_h = sizes[-1] // 2 + 1
+    half = [b] + sizes[:-1] + [last_h]
+    full = [b] + sizes
+    g = torch.Generator(device="cuda").manual_seed(7)
+    if kind == fft.ASCEND_FFT_C2C:
+        x = torch.randn(full, dtype=torch.complex64, device="cuda", generator=g)
+        y = torch.empty_like(x)
+        nbytes = 16 * n_total * b
+    elif kind == fft.ASCEND_FFT_R2C:
+        x = torch.randn(full, dtype=torch.float32, device="cuda", generator=g)
+        y = torch.empty(half, dtype=torch.complex64, device="cuda")
+        nbytes = (4 * n_total + 8 * n_total // sizes[-1] * last_h) * b
+    else:
+        x = torch.randn(half, dtype=torch.complex64, device="cuda", generator=g)
+        y = torch.empty(full, dtype=torch.float32, device="cuda")
+        nbytes = (4 * n_total + 8 * n_total // sizes[-1] * last_h) * b
+    plan = fft.FftPlan(sizes, kind, direction, b)
+    for _ in range(max(1, args.warmup)):
+        plan(x, y)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        plan(x, y)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    med = statistics.median(ms)
+    peak, pk = measured_peak_hbm()
+    acc = None
+    if args.check:
+        from oracle import oracle as _oracle  # checker only
+
+        nd = len(sizes)
+        xs, ys = x[:1].cpu().numpy(), y[:1].cpu().numpy()
+        f = direction == fft.ASCEND_FFT_FORWARD
+        ref = (_oracle.c2c(xs, f, ndim=nd) if kind == fft.ASCEND_FFT_C2C else
+               _oracle.r2c(xs, f, ndim=nd) if kind == fft.ASCEND_FFT_R2C else
+               _oracle.c2r(xs, sizes[-1], f, ndim=nd))
+        acc = {"rel_l2": _oracle.rel_l2(ys, ref), "bound": _oracle.tolerance(n_total)}
+    if rank == 0:
+        print(json.dumps({
+            "workload": f"{args.kind} sizes={sizes} batch={b} {'inverse' if args.inverse else 'forward'}",
+            "ms_median": med, "ms_min": min(ms), "GBps": nbytes / (med / 1e3) / 1e9,
+            "frac_of_hbm": nbytes / (med / 1e3) / 1e9 / peak, "peak_source": pk,
+            "GFLOPps": 5.0 * n_total * math.log2(max(2, n_total)) * b / (med / 1e3) / 1e9,
+            "launches": plan.launches(), "plan": plan.describe(), "accuracy": acc}), flush=True)
+    plan.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -515,7 +581,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="roundtrip", choices=["roundtrip", "uneven", "serving"])
+    ap.add_argument("--workload", default="roundtrip", choices=["roundtrip", "uneven", "serving", "kernel"])
+    ap.add_argument("--kind", default="c2c", choices=["c2c", "r2c", "c2r"], help="(kernel) transform type")
+    ap.add_argument("--sizes", default="4096", help="(kernel) comma-separated transform sizes (1D/2D/3D)")
+    ap.add_argument("--batch", type=int, default=4096, help="(kernel) batch")
+    ap.add_argument("--inverse", action="store_true", help="(kernel) INVERSE direction")
+    ap.add_argument("--check", action="store_true", help="(kernel) check one transform against the oracle")
     ap.add_argument("--device-io", action="store_true", help="(serving) request buffers in HBM instead of pinned host")
     ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--rates", default="1,10,100,1000,10000,50000")
@@ -529,6 +600,9 @@ def main():
         return
     if args.workload == "serving":
         run_serving(args, world, rank, local)
+        return
+    if args.workload == "kernel":
+        run_kernel(args, world, rank, local)
         return
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -124,6 +124,8 @@ cudaError_t configure_kernels(int device)
         cudaError_t e = allow_max_dynamic_smem(fn);
         if (e != cudaSuccess) return e;
     }
+    // the error word is allocated here, at set-up, never inside a capture
+    if (!device_error_word(device)) return cudaErrorMemoryAllocation;
     done[device] = true;
     return cudaSuccess;
 }
