@@ -21,17 +21,10 @@
 #include "codelets.cuh"
 #include "fft_tile.cuh"
 #include "sipfft_internal.h"
+#include "tile_io.cuh"
 
 namespace sipfft {
 
-__device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
-
-__device__ __forceinline__ int64_t col_base(const Addr &a, int64_t o, int64_t c)
-{
-    int64_t x = o * a.dist + c * a.cstride;
-    if (a.cblock) x += (c / a.cblock) * a.cjump;
-    return x;
-}
 
 // Register budget of one stage: NB butterflies of radix R per thread.
 template <int R, int MAXE>
@@ -118,186 +111,6 @@ __device__ __forceinline__ void run_stages(float2 *row, const TileDesc &d, int l
     }
 }
 
-template <bool FWD>
-__device__ __forceinline__ float2 pass_twiddle(const TileDesc &d, int64_t e, int64_t kc)
-{
-    const int64_t m = e * kc * d.g_step;
-    const int64_t mask = (int64_t(1) << d.g_log2l) - 1;
-    const float2 w = cmul(__ldg(d.g_lo + (m & mask)), __ldg(d.g_hi + (m >> d.g_log2l)));
-    return dir<FWD>(w);
-}
-
-// ------------------------------------------------------------------------------------ load
-template <bool FWD>
-__device__ __forceinline__ void load_tile(const TileDesc &d, const void *in, float2 *sm, int64_t o, int64_t c0,
-                                          int ntr)
-{
-    const int tid = threadIdx.x, bd = blockDim.x;
-    const int n = d.n, P = d.pitch;
-    const int io = d.io;
-    if (io == IO_C2R_PACKED) {
-        // pairs (k, n-k) of the half spectrum -> packed n-point input
-        const int l = tid / d.tpt, lane = tid % d.tpt;
-        if (l >= ntr) return;
-        const float2 *x = static_cast<const float2 *>(in) + col_base(d.in_a, o, c0 + l);
-        float2 *row = sm + l * P;
-        for (int k = lane; 2 * k <= n; k += d.tpt) {
-            float2 xk = x[k];
-            float2 xm = x[n - k];
-            if (k == 0) {
-                xk.y = 0.f;
-                xm.y = 0.f;
-            }
-            const float2 e = cadd(xk, cconj(xm));
-            const float2 w = dir<FWD>(__ldg(d.tw + k));
-            const float2 od = cmul(csub(xk, cconj(xm)), w);
-            // Z[k] = e + i*od ; Z[n-k] = conj(e) + i*conj(od)
-            row[pad(k)] = make_float2(e.x - od.y, e.y + od.x);
-            if (k != 0 && 2 * k != n) row[pad(n - k)] = make_float2(e.x + od.y, -e.y + od.x);
-        }
-        return;
-    }
-    if (io == IO_BLUE_PRE) {
-        const int l = tid / d.tpt, lane = tid % d.tpt;
-        if (l >= ntr) return;
-        const int64_t base = col_base(d.in_a, o, c0 + l);
-        float2 *row = sm + l * P;
-        const int nb = d.blue_n;
-        for (int e = lane; e < n; e += d.tpt) {
-            float2 v = make_float2(0.f, 0.f);
-            if (e < nb) {
-                if (d.blue_kind == 1) {
-                    v = make_float2(static_cast<const float *>(in)[base + e], 0.f);
-                } else if (d.blue_kind == 2) {
-                    const float2 *x = static_cast<const float2 *>(in) + base;
-                    if (2 * e <= nb) {
-                        v = x[e];
-                        if (e == 0 || 2 * e == nb) v.y = 0.f;
-                    } else {
-                        v = cconj(x[nb - e]);
-                    }
-                } else {
-                    v = static_cast<const float2 *>(in)[base + e];
-                }
-                v = cmul(v, __ldg(d.chirp + e));
-            }
-            row[pad(e)] = v;
-        }
-        return;
-    }
-    if (io == IO_C2R_FULL) {
-        const int l = tid / d.tpt, lane = tid % d.tpt;
-        if (l >= ntr) return;
-        const float2 *x = static_cast<const float2 *>(in) + col_base(d.in_a, o, c0 + l);
-        float2 *row = sm + l * P;
-        for (int k = lane; 2 * k <= n; k += d.tpt) {
-            float2 xk = x[k];
-            if (k == 0) xk.y = 0.f;
-            row[pad(k)] = xk;
-            if (k != 0) row[pad(n - k)] = cconj(xk);
-        }
-        return;
-    }
-    // element-wise kinds: C2C, R2C_PACKED (float pairs), R2C_FULL (floats)
-    const bool contiguous = d.in_a.estride == 1;
-    int l, e0, estep;
-    if (contiguous) {
-        l = tid / d.tpt;
-        e0 = tid % d.tpt;
-        estep = d.tpt;
-    } else {
-        l = tid % d.tb;
-        e0 = tid / d.tb;
-        estep = bd / d.tb;
-    }
-    if (l >= ntr) return;
-    const int64_t base = col_base(d.in_a, o, c0 + l);
-    const int64_t es = d.in_a.estride;
-    float2 *row = sm + l * P;
-    if (io == IO_R2C_FULL) {
-        const float *x = static_cast<const float *>(in) + base;
-        for (int e = e0; e < n; e += estep) row[pad(e)] = make_float2(x[e * es], 0.f);
-        return;
-    }
-    const float2 *x = static_cast<const float2 *>(in) + base;
-    if (d.g_twiddle) {
-        const int64_t kc = (c0 + l) % d.g_ns;
-        for (int e = e0; e < n; e += estep) row[pad(e)] = cmul(x[e * es], pass_twiddle<FWD>(d, e, kc));
-    } else {
-        for (int e = e0; e < n; e += estep) row[pad(e)] = x[e * es];
-    }
-}
-
-// ------------------------------------------------------------------------------------ store
-template <bool FWD>
-__device__ __forceinline__ void store_tile(const TileDesc &d, void *out, const float2 *sm, int64_t o, int64_t c0,
-                                           int ntr)
-{
-    const int tid = threadIdx.x, bd = blockDim.x;
-    const int n = d.n, P = d.pitch;
-    const int io = d.io;
-    if (io == IO_R2C_PACKED) {
-        const int l = tid / d.tpt, lane = tid % d.tpt;
-        if (l >= ntr) return;
-        float2 *y = static_cast<float2 *>(out) + col_base(d.out_a, o, c0 + l);
-        const float2 *row = sm + l * P;
-        for (int k = lane; 2 * k <= n; k += d.tpt) {
-            const float2 zk = row[pad(k)];
-            const float2 zm = cconj(row[pad(k == 0 ? 0 : n - k)]);
-            const float2 e = cscale(cadd(zk, zm), 0.5f);
-            const float2 t = csub(zk, zm);
-            const float2 od = make_float2(0.5f * t.y, -0.5f * t.x);  // -i/2 * t
-            const float2 wo = cmul(dir<FWD>(__ldg(d.tw + k)), od);
-            y[k] = cadd(e, wo);
-            if (2 * k != n) y[n - k] = cconj(csub(e, wo));
-        }
-        return;
-    }
-    if (io == IO_BLUE_PRE || io == IO_BLUE_POST) {
-        const int l = tid / d.tpt, lane = tid % d.tpt;
-        if (l >= ntr) return;
-        const int64_t base = col_base(d.out_a, o, c0 + l);
-        const float2 *row = sm + l * P;
-        if (io == IO_BLUE_PRE) {
-            float2 *y = static_cast<float2 *>(out) + base;
-            for (int e = lane; e < n; e += d.tpt) y[e] = cmul(row[pad(e)], __ldg(d.bmul + e));
-        } else if (d.blue_kind == 2) {
-            float *y = static_cast<float *>(out) + base;
-            for (int e = lane; e < d.blue_n; e += d.tpt) y[e] = cmul(row[pad(e)], __ldg(d.chirp + e)).x;
-        } else {
-            const int count = d.blue_kind == 1 ? d.blue_n / 2 + 1 : d.blue_n;
-            float2 *y = static_cast<float2 *>(out) + base;
-            for (int e = lane; e < count; e += d.tpt) y[e] = cmul(row[pad(e)], __ldg(d.chirp + e));
-        }
-        return;
-    }
-    const bool contiguous = d.out_a.estride == 1;
-    int l, e0, estep;
-    if (contiguous) {
-        l = tid / d.tpt;
-        e0 = tid % d.tpt;
-        estep = d.tpt;
-    } else {
-        l = tid % d.tb;
-        e0 = tid / d.tb;
-        estep = bd / d.tb;
-    }
-    if (l >= ntr) return;
-    const int64_t base = col_base(d.out_a, o, c0 + l);
-    const int64_t es = d.out_a.estride;
-    const float2 *row = sm + l * P;
-    if (io == IO_C2R_FULL) {
-        float *y = static_cast<float *>(out) + base;
-        for (int e = e0; e < n; e += estep) y[e * es] = row[pad(e)].x;
-        return;
-    }
-    const int count = (io == IO_R2C_FULL) ? n / 2 + 1 : n;
-    float2 *y = static_cast<float2 *>(out) + base;
-    for (int e = e0; e < count; e += estep) y[e * es] = row[pad(e)];
-}
-
-// One tile: load, Stockham stages, store.  Threads beyond tb*tpt (a launch
-// shared by tiles of different shapes) only take part in the barriers.
 template <int MAXE, bool FWD>
 __device__ __forceinline__ void process_tile(const TileDesc &d, const void *in, void *out, int64_t g, float2 *sm)
 {

@@ -19,7 +19,10 @@
 
 namespace sipfft {
 
+#ifndef SIPFFT_PAD_DEFINED
+#define SIPFFT_PAD_DEFINED
 __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+#endif
 
 template <int R, int MAXE>
 constexpr int nb_for() { return (MAXE + R - 1) / R; }
