@@ -539,7 +539,9 @@ def run_kernel(args, world, rank, local):
         x = torch.randn(half, dtype=torch.complex64, device="cuda", generator=g)
         y = torch.empty(full, dtype=torch.float32, device="cuda")
         nbytes = (4 * n_total + 8 * n_total // sizes[-1] * last_h) * b
-    plan = fft.FftPlan(sizes, kind, direction, b)
+    precision = {"fp32": fft.PRECISION_FP32, "fp16x3": fft.PRECISION_FP16X3,
+                 "bf16x3": fft.PRECISION_BF16X3}[args.precision]
+    plan = fft.FftPlan(sizes, kind, direction, b, precision=precision)
     plan(x, y)  # through the aclTensor entry point once (shape checks)
     # then back-to-back raw-pointer executions, so host overhead does not
     # open gaps between launches inside the timed region
@@ -572,6 +574,7 @@ def run_kernel(args, world, rank, local):
     if rank == 0:
         print(json.dumps({
             "workload": f"{args.kind} sizes={sizes} batch={b} {'inverse' if args.inverse else 'forward'}",
+            "precision": args.precision,
             "ms_median": med, "ms_min": min(ms), "GBps": nbytes / (med / 1e3) / 1e9,
             "frac_of_hbm": nbytes / (med / 1e3) / 1e9 / peak, "peak_source": pk,
             "GFLOPps": 5.0 * n_total * math.log2(max(2, n_total)) * b / (med / 1e3) / 1e9,
@@ -593,6 +596,8 @@ def main():
     ap.add_argument("--inverse", action="store_true", help="(kernel) INVERSE direction")
     ap.add_argument("--check", action="store_true", help="(kernel) check one transform against the oracle")
     ap.add_argument("--reps", type=int, default=20, help="(kernel) executions per timed sample")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16x3", "bf16x3"],
+                    help="(kernel) stage arithmetic: FP32 kernels or tensor-core hi/lo split forms")
     ap.add_argument("--device-io", action="store_true", help="(serving) request buffers in HBM instead of pinned host")
     ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--rates", default="1,10,100,1000,10000,50000")

@@ -28,6 +28,18 @@ ASDSIP_API int64_t asdFftGetErrorMessage(char *buf, int64_t len);
 /* Number of kernel launches one execution of the plan issues. */
 ASDSIP_API int32_t asdFftPlanLaunchCount(void *handle);
 
+/* ---- arithmetic of the transform stages.  No counterpart in the reference (its cores are FP32 only).
+ * mode 0: FP32 CUDA-core kernels (default).
+ * mode 1: tensor-core (tcgen05) DFT-matrix stages, operands split into FP16 hi + lo parts with a
+ *         power-of-two scale per tile, three products hi*hi + hi*lo + lo*hi accumulated in FP32.
+ * mode 2: the same with BF16 hi + lo parts (no scaling; about 16 significant bits per operand).
+ * Tensor-core stages exist for transform lengths 1024, 2048 and 4096 of a C2C axis (and 2048, 4096 and
+ * 8192 for R2C / C2R, whose packed inner transform has half the length); every other step keeps the FP32
+ * kernels, which asdFftDescribePlan shows.  May be called before or after MakePlan*: an initialised
+ * plan is rebuilt (the workspace size does not change).  Returns ACL_ERROR_INVALID_PARAM for an unknown
+ * handle or mode. */
+ASDSIP_API int32_t asdFftSetPrecision(void *handle, int32_t mode);
+
 /* ---- uneven batches: many 1D C2C groups (length sizes[i], count batches[i]) stored back to back,
  * executed by ONE persistent kernel launch (optionally replayed from a captured CUDA graph).
  * tune_cache: optional path of the autotuner's cache (choices for this GPU are loaded). */

@@ -510,6 +510,30 @@ int64_t asdFftGetErrorMessage(char *buf, int64_t len)
     return static_cast<int64_t>(s.size()) + 1;
 }
 
+int32_t asdFftSetPrecision(void *handle, int32_t mode)
+{
+    sipfft::Plan *p = find_plan(handle);
+    if (!p || mode < 0 || mode > 2) {
+        log_error("asdFftSetPrecision", "unknown handle or precision mode");
+        return AsdSip::ACL_ERROR_INVALID_PARAM;
+    }
+    std::lock_guard<std::mutex> lock(p->mu);
+    if (p->precision == mode) return AsdSip::ACL_SUCCESS;
+    p->precision = mode;
+    if (!p->initialized) return AsdSip::ACL_SUCCESS;
+    const size_t ws = p->ws_bytes;
+    std::string (*builder)(sipfft::Plan &) = p->sizes.size() == 1   ? sipfft::build_plan_1d
+                                             : p->sizes.size() == 2 ? sipfft::build_plan_2d
+                                                                    : sipfft::build_plan_3d;
+    const AspbStatus st = finish_plan(*p, builder, "asdFftSetPrecision");
+    if (st == AsdSip::ACL_SUCCESS && p->ws_bytes > ws) {
+        p->initialized = false;
+        log_error("asdFftSetPrecision", "rebuilt plan needs a larger workspace");
+        return AsdSip::ACL_ERROR_INTERNAL_ERROR;
+    }
+    return st;
+}
+
 int32_t asdFftPlanLaunchCount(void *handle)
 {
     sipfft::Plan *p = find_plan(handle);

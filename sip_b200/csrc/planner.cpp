@@ -221,6 +221,46 @@ struct Builder {
         if (!column && n_outer == 1 && ia.estride == 1 && oa.estride == 1 &&
             (io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
             add_row_variant(s, c, ia.cstride, oa.cstride);
+        if (p.precision != 0 && (io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
+            return add_tc_variant(s);
+        return true;
+    }
+
+    // Tensor-core split-precision form of a tile step (lengths with a
+    // tcgen05 kernel); replaces the FP32 kernels of the step.
+    bool add_tc_variant(Step &s)
+    {
+        TcConfig tc;
+        const int n = s.d.n;
+        if (!tc_config(n, tc)) return true;
+        const int fmt = p.precision == 1 ? 0 : 1;
+        size_t smem = 0;
+        const void *fn = tc_kernel(n, fmt, s.forward, &smem);
+        if (!fn) return true;
+        TablePtr m1 = get_tc_matrix(tc.n1, fmt, fwd, device, &err);
+        if (!m1) return false;
+        TablePtr m2 = tc.n2 == tc.n1 ? m1 : get_tc_matrix(tc.n2, fmt, fwd, device, &err);
+        if (!m2) return false;
+        const float2 *tw = table(n, n);
+        if (!tw) return false;
+        p.tables.push_back(m1);
+        p.tables.push_back(m2);
+        TileDesc &d = s.d;
+        d.tb = tc.tb;
+        d.tpt = 128 / tc.tb;
+        d.pitch = ((n - 1) + ((n - 1) >> 4) + 1) | 1;
+        d.tiles_per_outer = (d.n_cols + d.tb - 1) / d.tb;
+        d.num_tiles = d.tiles_per_outer * d.n_outer;
+        const int per_sm = std::max(1, kernel_blocks_per_sm(fn, 128, smem));
+        s.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(d.num_tiles, int64_t(per_sm) * sm_count(device))));
+        s.has_row = false;
+        s.row_fn = nullptr;
+        s.tc_fmt = fmt;
+        s.tc_mat[0] = reinterpret_cast<const uint16_t *>(m1->ptr);
+        s.tc_mat[1] = reinterpret_cast<const uint16_t *>(m1->ptr + int64_t(64) * tc.n1);
+        s.tc_mat[2] = reinterpret_cast<const uint16_t *>(m2->ptr);
+        s.tc_mat[3] = reinterpret_cast<const uint16_t *>(m2->ptr + int64_t(64) * tc.n2);
+        s.tc_tw = tw;
         return true;
     }
 
@@ -671,6 +711,8 @@ std::string describe_plan(const Plan &p)
             for (int i = 0; i < s.d.nstages; i++) o << (i ? "x" : "") << s.d.radix[i];
             o << " tb=" << s.d.tb << " tpt=" << s.d.tpt << " tiles=" << s.d.num_tiles << " grid=" << s.grid
               << " smem=" << s.d.tb * s.d.pitch * 8;
+            if (s.tc_fmt >= 0)
+                o << " | tensor-core " << (s.tc_fmt == 0 ? "fp16x3" : "bf16x3") << " tb=" << s.d.tb << " grid=" << s.grid;
             if (s.has_row)
                 o << " | row-pipelined" << (s.row_fn ? " static" : "") << " tb=" << s.rd.tb << " tpt=" << s.rd.tpt
                   << " grid=" << s.row_grid << " smem=" << row_kernel_smem(s.rd);

@@ -82,6 +82,35 @@ TablePtr get_stage_table(const StaticKernel &k, int device, std::string *err)
     return t;
 }
 
+TablePtr get_tc_matrix(int N, int fmt, bool fwd, int device, std::string *err)
+{
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int>, std::weak_ptr<DeviceTable>> cache;  // (device, N, fmt, fwd)
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_tuple(device, N, fmt, fwd ? 1 : 0);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+        if (TablePtr t = it->second.lock()) return t;
+    }
+    auto t = std::make_shared<DeviceTable>();
+    t->count = int64_t(128) * N;  // hi + lo, 2 x (128 x 2N) 16-bit values
+    t->device = device;
+    cudaError_t e = cudaMalloc(&t->ptr, sizeof(float2) * static_cast<size_t>(t->count));
+    if (e == cudaSuccess) {
+        uint16_t *hi = reinterpret_cast<uint16_t *>(t->ptr);
+        uint16_t *lo = reinterpret_cast<uint16_t *>(t->ptr + int64_t(64) * N);
+        e = fill_tc_matrix(hi, lo, N, fmt, fwd, 0);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) {
+        if (err) *err = std::string("twiddle table: ") + cudaGetErrorString(e);
+        cudaGetLastError();
+        return nullptr;
+    }
+    cache[key] = t;
+    return t;
+}
+
 namespace {
 thread_local std::string t_last_error;
 }  // namespace
@@ -120,6 +149,7 @@ cudaError_t configure_kernels(int device)
     tile_kernel_fns(fns);
     row_kernel_fns(fns);
     static_kernel_fns(fns);
+    tc_kernel_fns(fns);
     for (const void *fn : fns) {
         cudaError_t e = allow_max_dynamic_smem(fn);
         if (e != cudaSuccess) return e;
@@ -199,7 +229,13 @@ cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const v
         cudaError_t e = cudaSuccess;
         switch (s.kind) {
             case StepKind::kTile: {
-                if (s.has_row && (reinterpret_cast<uintptr_t>(src) & 15) == 0 && src != dst) {
+                if (s.tc_fmt >= 0) {
+                    TileDesc d = s.d;
+                    d.in = src;
+                    d.out = dst;
+                    e = launch_tc(d, d.n, s.tc_fmt, s.forward, s.tc_mat, s.tc_tw, s.grid, device_error_word(p.device),
+                                  st);
+                } else if (s.has_row && (reinterpret_cast<uintptr_t>(src) & 15) == 0 && src != dst) {
                     TileDesc d = s.rd;
                     d.in = src;
                     d.out = dst;

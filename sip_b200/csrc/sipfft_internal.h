@@ -57,6 +57,19 @@ struct StaticKernel {
 const StaticKernel *find_static_kernel(int n, int io);
 cudaError_t fill_stage_twiddles(float2 *t, const int *radix, int nstages, cudaStream_t st);
 int64_t stage_twiddle_count(const int *radix, int nstages);
+// Tensor-core split-precision stages (tc_fft.cu): n = n1 * n2 as two DFT-matrix
+// GEMMs on tcgen05 with hi/lo FP16 or BF16 operands and FP32 accumulation.
+// fmt 0 = FP16 x3 (per-tile power-of-two scaling), 1 = BF16 x3.
+struct TcConfig {
+    int n1 = 0, n2 = 0, tb = 0;  // tb transforms per CTA (128 threads)
+};
+bool tc_config(int n, TcConfig &c);
+const void *tc_kernel(int n, int fmt, bool fwd, size_t *smem);
+void tc_kernel_fns(std::vector<const void *> &out);
+// 128 x 2N real DFT matrix of one stage in the operand layout, hi and lo parts
+cudaError_t fill_tc_matrix(uint16_t *hi, uint16_t *lo, int N, int fmt, bool fwd, cudaStream_t st);
+cudaError_t launch_tc(const TileDesc &d, int n, int fmt, bool fwd, const uint16_t *const *mats, const float2 *tw,
+                      int grid, int *err, cudaStream_t st);
 // Process-wide device error word of the current device (bounded waits that
 // gave up set it); read and cleared by asdFftSynchronize.
 int *device_error_word(int device);
@@ -84,6 +97,9 @@ using TablePtr = std::shared_ptr<DeviceTable>;
 TablePtr get_table(int64_t count, int64_t denom, int64_t mult, int device, std::string *err);
 // per-stage twiddle tables of a static kernel's radix sequence
 TablePtr get_stage_table(const StaticKernel &k, int device, std::string *err);
+// hi/lo operand matrices of one tensor-core stage (N points, fmt, direction):
+// hi at ptr, lo at ptr + 64 N float2 (each 128 x 2N 16-bit values)
+TablePtr get_tc_matrix(int N, int fmt, bool fwd, int device, std::string *err);
 
 enum class Buf : int { kUserIn = 0, kUserOut = 1, kWs0 = 2, kWs1 = 3 };
 
@@ -104,6 +120,10 @@ struct Step {
     TileDesc rd{};
     int row_grid = 1;
     const void *row_fn = nullptr;
+    // tensor-core variant (tc_fmt >= 0): d is launched by launch_tc with these matrices
+    int tc_fmt = -1;
+    const uint16_t *tc_mat[4] = {};  // stage-1 hi, lo, stage-2 hi, lo
+    const float2 *tc_tw = nullptr;
     // kR2CPost / kC2RPre
     int64_t rows = 0, m = 0, src_dist = 0, dst_dist = 0;
     const float2 *lo = nullptr, *hi = nullptr;
@@ -140,6 +160,9 @@ struct Plan {
     bool use_tuned = false;  // consult the autotuner's choices (uneven-batch plans)
     int row_threads = 256;   // threads per CTA the row tiles aim for
     int row_smem = 64 * 1024;  // shared memory per CTA the row tiles stay under
+    // 0: FP32 kernels; 1: tensor-core FP16 hi/lo x3; 2: tensor-core BF16 hi/lo x3
+    // (lengths without a tensor-core stage keep the FP32 kernels)
+    int precision = 0;
     bool forward() const;
 };
 

@@ -44,6 +44,11 @@ ASCEND_FFT_INVERSE = 0x11
 ASCEND_FFT_HORIZONTAL = 0x10
 ASCEND_FFT_VERTICAL = 0x11
 
+# asdFftSetPrecision modes (arithmetic of the transform stages)
+PRECISION_FP32 = 0       # CUDA-core FP32 kernels
+PRECISION_FP16X3 = 1     # tensor-core DFT-matrix stages, FP16 hi/lo split, 3 products, FP32 accumulate
+PRECISION_BF16X3 = 2     # the same with BF16 hi/lo parts
+
 ACL_FLOAT = 0
 ACL_COMPLEX64 = 16
 ACL_FORMAT_ND = 2
@@ -60,7 +65,7 @@ EXPORTED_SYMBOLS = (
     "asdFftBatchDescribe", "asdFftAutotune", "asdFftTuneCacheLoad",
     "asdFftServerCreate", "asdFftServerWarm", "asdFftServerSubmit", "asdFftServerDrain", "asdFftServerBatches",
     "asdFftServerDestroy", "asdFftServeRun", "asdFftServerHold", "asdFftGetErrorMessage",
-    "asdFftExecC2CNoAlloc",
+    "asdFftExecC2CNoAlloc", "asdFftSetPrecision",
 )
 
 
@@ -122,6 +127,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "asdFftExecRaw": (i32, [vp, vp, vp]),
         "asdFftDescribePlan": (i64, [vp, ctypes.c_char_p, i64]),
         "asdFftPlanLaunchCount": (i32, [vp]),
+        "asdFftSetPrecision": (i32, [vp, i32]),
         "asdFftBatchPlanCreate": (i32, [ctypes.POINTER(vp), P64, P64, i32, i32, ctypes.c_char_p]),
         "asdFftBatchGetWorkspaceSize": (i32, [vp, ctypes.POINTER(sz)]),
         "asdFftBatchExec": (i32, [vp, vp, vp, vp, vp, i32]),
@@ -280,14 +286,21 @@ class FftPlan:
     """Handle + plan + workspace; executes on torch CUDA tensors through the aclTensor entry points."""
 
     def __init__(self, sizes: Sequence[int], fft_type: int, direction: int, batch: int,
-                 dim_type: int = ASCEND_FFT_HORIZONTAL, stream=None):
+                 dim_type: int = ASCEND_FFT_HORIZONTAL, stream=None, precision: int = PRECISION_FP32):
         import torch
 
         self.sizes = [int(s) for s in sizes]
         self.fft_type = fft_type
         self.direction = direction
         self.batch = int(batch)
+        self.precision = int(precision)
         self.handle = asdFftCreate()
+        if self.precision != PRECISION_FP32:
+            st = load_library().asdFftSetPrecision(self.handle, self.precision)
+            if st != ACL_SUCCESS:
+                asdFftDestroy(self.handle)
+                self.handle = None
+                raise FftError("asdFftSetPrecision", st)
         if len(sizes) == 1:
             st = asdFftMakePlan1D(self.handle, self.sizes[0], fft_type, direction, self.batch, dim_type)
         elif len(sizes) == 2:

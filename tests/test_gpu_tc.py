@@ -1,0 +1,139 @@
+"""GPU parity of the tensor-core split-precision stages (asdFftSetPrecision
+modes 1 = FP16 hi/lo x3 and 2 = BF16 hi/lo x3) against the FP64 oracle.
+
+Bar: relative L2 error <= 1e-6 * log2(N), the FP32 gate of the path.  The
+FP16 form must also agree with the numpy replay of the kernel
+(tests/tc_model.py) to 2e-6: the tensor cores' FP32 accumulation does not
+round like the replay's (measured differences about 7e-7), but a wrong operand
+layout or scale would show as an O(1) difference.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from sip_b200 import fft
+
+import tc_model
+
+pytestmark = pytest.mark.gpu
+
+C2C, R2C, C2R = fft.ASCEND_FFT_C2C, fft.ASCEND_FFT_R2C, fft.ASCEND_FFT_C2R
+FWD, INV = fft.ASCEND_FFT_FORWARD, fft.ASCEND_FFT_INVERSE
+MODES = [fft.PRECISION_FP16X3, fft.PRECISION_BF16X3]
+
+
+def _rand_complex(rng, shape):
+    return (rng.uniform(-1, 1, shape) + 1j * rng.uniform(-1, 1, shape)).astype(np.complex64)
+
+
+def _run(sizes, typ, direction, batch, x, precision, dim_type=fft.ASCEND_FFT_HORIZONTAL, inplace=False):
+    import torch
+
+    plan = fft.FftPlan(sizes, typ, direction, batch, dim_type, precision=precision)
+    try:
+        desc = plan.describe()
+        xin = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+        if inplace:
+            out = xin
+        elif typ == C2C:
+            out = torch.empty_like(xin)
+        elif typ == R2C:
+            out = torch.empty(x.shape[:-1] + (sizes[-1] // 2 + 1,), dtype=torch.complex64, device="cuda")
+        else:
+            out = torch.empty(x.shape[:-1] + (sizes[-1],), dtype=torch.float32, device="cuda")
+        plan(xin, out)
+        torch.cuda.synchronize()
+        assert fft.asdFftSynchronize(plan.handle) == fft.ACL_SUCCESS
+        return out.cpu().numpy(), desc
+    finally:
+        plan.close()
+
+
+@pytest.mark.parametrize("precision", MODES, ids=["fp16x3", "bf16x3"])
+@pytest.mark.parametrize("direction", [FWD, INV], ids=["fwd", "inv"])
+@pytest.mark.parametrize("n", [1024, 2048, 4096])
+def test_c2c_rows(cuda, n, direction, precision):
+    tb = tc_model.CONFIGS[n][2]
+    batch = 37 * tb + 1  # several tiles per CTA and one partial tile
+    rng = np.random.default_rng(n + precision)
+    x = _rand_complex(rng, (batch, n))
+    y, desc = _run([n], C2C, direction, batch, x, precision)
+    assert "tensor-core" in desc, desc
+    f = direction == FWD
+    err = oracle.rel_l2(y, oracle.c2c(x, f))
+    assert err <= oracle.tolerance(n), (err, desc)
+    if precision == fft.PRECISION_FP16X3:
+        model = tc_model.tc_fft(x[:2 * tb + 1], f, 0)
+        assert oracle.rel_l2(y[:2 * tb + 1], model) <= 2e-6
+
+
+@pytest.mark.parametrize("precision", MODES, ids=["fp16x3", "bf16x3"])
+def test_c2c_inplace_and_scaled_inputs(cuda, precision):
+    rng = np.random.default_rng(11)
+    x = (_rand_complex(rng, (9, 1024)) * np.float32(3e4)).astype(np.complex64)
+    y, _ = _run([1024], C2C, FWD, 9, x, precision, inplace=True)
+    assert oracle.rel_l2(y, oracle.c2c(x, True)) <= oracle.tolerance(1024)
+
+
+@pytest.mark.parametrize("precision", MODES, ids=["fp16x3", "bf16x3"])
+def test_c2c_vertical_columns(cuda, precision):
+    n, batch = 2048, 40
+    rng = np.random.default_rng(3)
+    x = _rand_complex(rng, (n, batch))
+    y, desc = _run([n], C2C, FWD, batch, x, precision, fft.ASCEND_FFT_VERTICAL)
+    assert "tensor-core" in desc, desc
+    assert oracle.rel_l2(y, oracle.c2c(x.T, True).T) <= oracle.tolerance(n)
+
+
+@pytest.mark.parametrize("precision", MODES, ids=["fp16x3", "bf16x3"])
+@pytest.mark.parametrize("direction", [FWD, INV], ids=["fwd", "inv"])
+@pytest.mark.parametrize("n", [4096, 8192])
+def test_real_transforms(cuda, n, direction, precision):
+    rng = np.random.default_rng(n + direction)
+    batch = 33
+    f = direction == FWD
+    xr = rng.standard_normal((batch, n)).astype(np.float32)
+    y, desc = _run([n], R2C, direction, batch, xr, precision)
+    assert "tensor-core" in desc, desc
+    assert oracle.rel_l2(y, oracle.r2c(xr, f)) <= oracle.tolerance(n)
+    h = n // 2 + 1
+    xh = (rng.standard_normal((batch, h)) + 1j * rng.standard_normal((batch, h))).astype(np.complex64)
+    y, desc = _run([n], C2R, direction, batch, xh, precision)
+    assert "tensor-core" in desc, desc
+    assert oracle.rel_l2(y, oracle.c2r(xh, n, f)) <= oracle.tolerance(n)
+
+
+@pytest.mark.parametrize("precision", MODES, ids=["fp16x3", "bf16x3"])
+def test_2d_2048(cuda, precision):
+    rng = np.random.default_rng(8)
+    x = _rand_complex(rng, (2, 2048, 2048))
+    y, desc = _run([2048, 2048], C2C, FWD, 2, x, precision)
+    assert desc.count("tensor-core") == 2, desc
+    assert oracle.rel_l2(y, oracle.c2c(x, True, ndim=2)) <= oracle.tolerance(2048 * 2048)
+
+
+def test_fp32_default_has_no_tensor_core_step(cuda):
+    rng = np.random.default_rng(1)
+    x = _rand_complex(rng, (4, 1024))
+    y, desc = _run([1024], C2C, FWD, 4, x, fft.PRECISION_FP32)
+    assert "tensor-core" not in desc
+    assert oracle.rel_l2(y, oracle.c2c(x, True)) <= oracle.tolerance(1024)
+
+
+def test_set_precision_after_plan_rebuilds(cuda):
+    import torch
+
+    plan = fft.FftPlan([2048], C2C, FWD, 8)
+    try:
+        assert "tensor-core" not in plan.describe()
+        assert fft.load_library().asdFftSetPrecision(plan.handle, fft.PRECISION_FP16X3) == fft.ACL_SUCCESS
+        assert "tensor-core fp16x3" in plan.describe()
+        rng = np.random.default_rng(2)
+        x = _rand_complex(rng, (8, 2048))
+        xin = torch.from_numpy(x).cuda()
+        out = torch.empty_like(xin)
+        plan(xin, out)
+        torch.cuda.synchronize()
+        assert oracle.rel_l2(out.cpu().numpy(), oracle.c2c(x, True)) <= oracle.tolerance(2048)
+    finally:
+        plan.close()
