@@ -232,6 +232,35 @@ struct Builder {
     {
         TcConfig tc;
         const int n = s.d.n;
+        const int fmt_rows = p.precision == 1 ? 0 : 1;
+        if (s.d.io == IO_C2C && !s.d.xfast && s.d.n_outer == 1 && s.d.in_a.estride == 1 && s.d.out_a.estride == 1 &&
+            tc_rows_config(n, tc)) {
+            // contiguous C2C rows: the warp-specialised row pipeline
+            size_t smem = 0;
+            const void *fn = tc_rows_kernel_fn(n, fmt_rows, s.forward, &smem);
+            if (fn) {
+                TablePtr fa = get_tc_matrix(tc.n1, fmt_rows, fwd, device, &err, 1);
+                if (!fa) return false;
+                TablePtr fb = tc.n2 == tc.n1 ? fa : get_tc_matrix(tc.n2, fmt_rows, fwd, device, &err, 1);
+                if (!fb) return false;
+                const float2 *tw = table(n, n);
+                if (!tw) return false;
+                p.tables.push_back(fa);
+                p.tables.push_back(fb);
+                const int64_t tiles = (s.d.n_cols + tc.tb - 1) / tc.tb;
+                const int per_sm = std::max(1, kernel_blocks_per_sm(fn, 416, smem));
+                s.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(per_sm) * sm_count(device))));
+                s.d.tb = tc.tb;
+                s.has_row = false;
+                s.row_fn = nullptr;
+                s.tc_fmt = fmt_rows;
+                s.tc_kind = 1;
+                s.tc_mat[0] = reinterpret_cast<const uint16_t *>(fa->ptr);
+                s.tc_mat[1] = reinterpret_cast<const uint16_t *>(fb->ptr);
+                s.tc_tw = tw;
+                return true;
+            }
+        }
         if (!tc_config(n, tc)) return true;
         const int fmt = p.precision == 1 ? 0 : 1;
         size_t smem = 0;
@@ -712,7 +741,8 @@ std::string describe_plan(const Plan &p)
             o << " tb=" << s.d.tb << " tpt=" << s.d.tpt << " tiles=" << s.d.num_tiles << " grid=" << s.grid
               << " smem=" << s.d.tb * s.d.pitch * 8;
             if (s.tc_fmt >= 0)
-                o << " | tensor-core " << (s.tc_fmt == 0 ? "fp16x3" : "bf16x3") << " tb=" << s.d.tb << " grid=" << s.grid;
+                o << " | tensor-core " << (s.tc_fmt == 0 ? "fp16x3" : "bf16x3") << (s.tc_kind == 1 ? " rows" : " tile")
+                  << " tb=" << s.d.tb << " grid=" << s.grid;
             if (s.has_row)
                 o << " | row-pipelined" << (s.row_fn ? " static" : "") << " tb=" << s.rd.tb << " tpt=" << s.rd.tpt
                   << " grid=" << s.row_grid << " smem=" << row_kernel_smem(s.rd);

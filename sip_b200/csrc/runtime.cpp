@@ -82,24 +82,27 @@ TablePtr get_stage_table(const StaticKernel &k, int device, std::string *err)
     return t;
 }
 
-TablePtr get_tc_matrix(int N, int fmt, bool fwd, int device, std::string *err)
+TablePtr get_tc_matrix(int N, int fmt, bool fwd, int device, std::string *err, int layout)
 {
     static std::mutex mu;
-    static std::map<std::tuple<int, int, int, int>, std::weak_ptr<DeviceTable>> cache;  // (device, N, fmt, fwd)
+    // (device, N, fmt, fwd, layout)
+    static std::map<std::tuple<int, int, int, int, int>, std::weak_ptr<DeviceTable>> cache;
     std::lock_guard<std::mutex> lock(mu);
-    auto key = std::make_tuple(device, N, fmt, fwd ? 1 : 0);
+    auto key = std::make_tuple(device, N, fmt, fwd ? 1 : 0, layout);
     auto it = cache.find(key);
     if (it != cache.end()) {
         if (TablePtr t = it->second.lock()) return t;
     }
     auto t = std::make_shared<DeviceTable>();
-    t->count = int64_t(128) * N;  // hi + lo, 2 x (128 x 2N) 16-bit values
+    // hi + lo 16-bit parts: 2 x (128 x 2N) (layout 0) or 2 x (2N x 2N) (layout 1)
+    const int64_t half = layout == 0 ? int64_t(64) * N : int64_t(N) * N;  // float2 units: 8 N^2 bytes per part
+    t->count = 2 * half;
     t->device = device;
     cudaError_t e = cudaMalloc(&t->ptr, sizeof(float2) * static_cast<size_t>(t->count));
     if (e == cudaSuccess) {
         uint16_t *hi = reinterpret_cast<uint16_t *>(t->ptr);
-        uint16_t *lo = reinterpret_cast<uint16_t *>(t->ptr + int64_t(64) * N);
-        e = fill_tc_matrix(hi, lo, N, fmt, fwd, 0);
+        uint16_t *lo = reinterpret_cast<uint16_t *>(t->ptr + half);
+        e = layout == 0 ? fill_tc_matrix(hi, lo, N, fmt, fwd, 0) : fill_tc_bmatrix(hi, lo, N, fmt, fwd, 0);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
@@ -150,6 +153,7 @@ cudaError_t configure_kernels(int device)
     row_kernel_fns(fns);
     static_kernel_fns(fns);
     tc_kernel_fns(fns);
+    tc_rows_kernel_fns(fns);
     for (const void *fn : fns) {
         cudaError_t e = allow_max_dynamic_smem(fn);
         if (e != cudaSuccess) return e;
@@ -229,7 +233,11 @@ cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const v
         cudaError_t e = cudaSuccess;
         switch (s.kind) {
             case StepKind::kTile: {
-                if (s.tc_fmt >= 0) {
+                if (s.tc_fmt >= 0 && s.tc_kind == 1) {
+                    e = launch_tc_rows(s.d.n, s.tc_fmt, s.forward, static_cast<const float2 *>(src),
+                                       static_cast<float2 *>(dst), s.d.n_cols, s.d.in_a.cstride, s.d.out_a.cstride,
+                                       s.tc_mat[0], s.tc_mat[1], s.tc_tw, s.grid, device_error_word(p.device), st);
+                } else if (s.tc_fmt >= 0) {
                     TileDesc d = s.d;
                     d.in = src;
                     d.out = dst;

@@ -70,6 +70,15 @@ void tc_kernel_fns(std::vector<const void *> &out);
 cudaError_t fill_tc_matrix(uint16_t *hi, uint16_t *lo, int N, int fmt, bool fwd, cudaStream_t st);
 cudaError_t launch_tc(const TileDesc &d, int n, int fmt, bool fwd, const uint16_t *const *mats, const float2 *tw,
                       int grid, int *err, cudaStream_t st);
+// Warp-specialised tensor-core kernel for contiguous C2C rows (tc_rows.cu).
+bool tc_rows_config(int n, TcConfig &c);
+const void *tc_rows_kernel_fn(int n, int fmt, bool fwd, size_t *smem);
+void tc_rows_kernel_fns(std::vector<const void *> &out);
+// 2N x 2N B-operand DFT matrix of one stage (hi at hi, lo at lo)
+cudaError_t fill_tc_bmatrix(uint16_t *hi, uint16_t *lo, int N, int fmt, bool fwd, cudaStream_t st);
+cudaError_t launch_tc_rows(int n, int fmt, bool fwd, const float2 *in, float2 *out, int64_t rows, int64_t in_dist,
+                           int64_t out_dist, const uint16_t *fa, const uint16_t *fb, const float2 *tw, int grid,
+                           int *err, cudaStream_t st);
 // Process-wide device error word of the current device (bounded waits that
 // gave up set it); read and cleared by asdFftSynchronize.
 int *device_error_word(int device);
@@ -97,9 +106,11 @@ using TablePtr = std::shared_ptr<DeviceTable>;
 TablePtr get_table(int64_t count, int64_t denom, int64_t mult, int device, std::string *err);
 // per-stage twiddle tables of a static kernel's radix sequence
 TablePtr get_stage_table(const StaticKernel &k, int device, std::string *err);
-// hi/lo operand matrices of one tensor-core stage (N points, fmt, direction):
-// hi at ptr, lo at ptr + 64 N float2 (each 128 x 2N 16-bit values)
-TablePtr get_tc_matrix(int N, int fmt, bool fwd, int device, std::string *err);
+// hi/lo operand matrices of one tensor-core stage (N points, fmt, direction).
+// layout 0 (A operand of tc_fft_kernel): hi at ptr, lo at ptr + 64 N float2,
+// each 128 x 2N 16-bit values; layout 1 (B operand of tc_rows_kernel): hi at
+// ptr, lo at ptr + N^2 float2, each 2N x 2N 16-bit values.
+TablePtr get_tc_matrix(int N, int fmt, bool fwd, int device, std::string *err, int layout = 0);
 
 enum class Buf : int { kUserIn = 0, kUserOut = 1, kWs0 = 2, kWs1 = 3 };
 
@@ -122,6 +133,7 @@ struct Step {
     const void *row_fn = nullptr;
     // tensor-core variant (tc_fmt >= 0): d is launched by launch_tc with these matrices
     int tc_fmt = -1;
+    int tc_kind = 0;  // 0: tile kernel (any IO / layout), 1: row pipeline (contiguous C2C rows)
     const uint16_t *tc_mat[4] = {};  // stage-1 hi, lo, stage-2 hi, lo
     const float2 *tc_tw = nullptr;
     // kR2CPost / kC2RPre

@@ -5,6 +5,8 @@
 #include <cstdio>
 
 #include <cute/arch/mma_sm100_desc.hpp>
+#include <cute/atom/mma_traits_sm100.hpp>
+#include <cute/tensor.hpp>
 
 #include "tc_desc.cuh"
 
@@ -63,6 +65,53 @@ int main()
             bad++;
         }
     }
+    // CUTLASS's descriptor builder on the two operand layouts of the row pipeline
+    // (start address is not representable on the host; LBO / SBO / layout are)
+    {
+        using namespace cute;
+        half_t *p = reinterpret_cast<half_t *>(0x400);
+        // MN-major A operand, K = 128, padded SBO of 2064 bytes (1032 elements)
+        auto mn = make_layout(make_shape(make_shape(Int<8>{}, Int<16>{}), make_shape(Int<8>{}, Int<16>{})),
+                              make_stride(make_stride(Int<1>{}, Int<1032>{}), make_stride(Int<8>{}, Int<64>{})));
+        UMMA::SmemDescriptor dm = UMMA::make_umma_desc<UMMA::Major::MN>(make_tensor(make_smem_ptr(p), mn));
+        const uint64_t mine_mn = sipfft::umma_smem_desc(0, 128, 2064);
+        if ((uint64_t(dm) & ~uint64_t(0x3FFF)) != (mine_mn & ~uint64_t(0x3FFF))) {
+            std::printf("MN-major smem desc mismatch: cute %llx mine %llx\n", (unsigned long long)uint64_t(dm),
+                        (unsigned long long)mine_mn);
+            bad++;
+        }
+        // K-major B operand (DFT matrix), K = 128, packed
+        auto km = make_layout(make_shape(make_shape(Int<8>{}, Int<16>{}), make_shape(Int<8>{}, Int<16>{})),
+                              make_stride(make_stride(Int<8>{}, Int<1024>{}), make_stride(Int<1>{}, Int<64>{})));
+        UMMA::SmemDescriptor dk = UMMA::make_umma_desc<UMMA::Major::K>(make_tensor(make_smem_ptr(p), km));
+        const uint64_t mine_k = sipfft::umma_smem_desc(0, 128, 2048);
+        if ((uint64_t(dk) & ~uint64_t(0x3FFF)) != (mine_k & ~uint64_t(0x3FFF))) {
+            std::printf("K-major smem desc mismatch: cute %llx mine %llx\n", (unsigned long long)uint64_t(dk),
+                        (unsigned long long)mine_k);
+            bad++;
+        }
+    }
+    // MN-major operand: K groups LBO = 128 bytes apart, 8-row M groups SBO apart
+    for (int mn = 0; mn < 2; mn++) {
+        const auto c = mn ? cute::UMMA::make_instr_desc<cute::half_t, cute::half_t, float, 128, 128,
+                                                        cute::UMMA::Major::MN, cute::UMMA::Major::K>()
+                          : cute::UMMA::make_instr_desc<cute::bfloat16_t, cute::bfloat16_t, float, 128, 64,
+                                                        cute::UMMA::Major::MN, cute::UMMA::Major::K>();
+        const uint32_t mine = mn ? sipfft::umma_instr_desc(128, 128, 0, 1, 0) : sipfft::umma_instr_desc(128, 64, 1, 1, 0);
+        if (uint32_t(c) != mine) {
+            std::printf("MN-major instr desc mismatch: cute %x mine %x\n", uint32_t(c), mine);
+            bad++;
+        }
+    }
+    for (int m = 0; m < 128; m++)
+        for (int k = 0; k < 128; k++) {
+            const uint32_t sbo = 2064;
+            const uint32_t canon = (m / 8) * sbo + (k / 8) * 128 + (k % 8) * 16 + (m % 8) * 2;
+            if (sipfft::umma_offset_mn(m, k, sbo) != canon) {
+                std::printf("mn layout error m=%d k=%d\n", m, k);
+                bad++;
+            }
+        }
     // layout: element (r, k) sits at (r/8)*SBO + (k/8)*LBO + (r%8)*16 + (k%8)*2, every byte once
     for (int K : {64, 128}) {
         const int rows = 128;

@@ -166,6 +166,117 @@ def tc_tile(x: np.ndarray, forward: bool, fmt: int) -> np.ndarray:
     return out.reshape(TB, n)[:ntr].astype(np.complex64)
 
 
+# ---------------------------------------------------------------------------- row pipeline (tc_rows.cu)
+ROWS_CONFIGS = {1024: (32, 32, 4), 2048: (64, 32, 4), 4096: (64, 64, 2)}
+
+
+def umma_offset_mn(m, k, sbo):
+    return (m >> 3) * sbo + (k >> 3) * 128 + (k & 7) * 16 + (m & 7) * 2
+
+
+def rows_layout(n: int):
+    """TcRowShape of tc_rows.cu."""
+    N1, N2, TB = ROWS_CONFIGS[n]
+    KA, KB, RA, RB = 2 * N1, 2 * N2, TB * N2, TB * N1
+    CHA, CHB = RA // 128, RB // 128
+    DC = CHA * KA
+    SBO_A, SBO_B = KA * 16 + 1024 // N2, KB * 16 + 1024 // N1
+    A1, A2 = 16 * SBO_A, 16 * SBO_B
+    FA, FB = KA * KA * 2, KB * KB * 2
+    off_fa = 1024
+    off_fb = off_fa + 2 * FA
+    off_a1 = off_fb + (0 if N1 == N2 else 2 * FB)
+    off_a2 = off_a1 + 2 * CHA * A1
+    total = off_a2 + 2 * CHB * A2
+    return dict(N1=N1, N2=N2, TB=TB, KA=KA, KB=KB, RA=RA, RB=RB, CHA=CHA, CHB=CHB, DC=DC, SBO_A=SBO_A,
+                SBO_B=SBO_B, A1_CHUNK=A1, A2_CHUNK=A2, FA=FA, FB=FB, off_a1=off_a1, off_a2=off_a2, total=total,
+                tmem_cols=4 * DC)
+
+
+def check_rows_bounds(n: int) -> None:
+    L = rows_layout(n)
+    N1, N2, TB, KA, KB = L["N1"], L["N2"], L["TB"], L["KA"], L["KB"]
+    assert L["RA"] % 128 == 0 and L["RB"] % 128 == 0
+    assert L["CHA"] * KA == L["CHB"] * KB == L["DC"] and L["DC"] in (64, 128)
+    assert L["tmem_cols"] <= 512 and L["total"] <= SMEM_LIMIT and L["total"] > 0
+    # header (TcHeader: 12 x 8 + 4 + 4 + 16 + 64 bytes) fits before the matrices
+    assert 12 * 8 + 8 + 16 + 64 <= 1024
+    # loader: element pair (e, e+1), e even, of transform t -> rows r = t N2 + n2 (+1), K n1 and N1 + n1
+    q = np.arange(TB * n // 2)
+    t, e = q // (n // 2), 2 * (q % (n // 2))
+    n1, n2 = e // N2, e % N2
+    r = t * N2 + n2
+    ch, m = r >> 7, r & 127
+    assert ch.max() < L["CHA"]
+    for k in (n1, N1 + n1):
+        off = ch * L["A1_CHUNK"] + umma_offset_mn(m, k, L["SBO_A"])
+        assert off.min() >= 0 and (off + 4).max() <= L["CHA"] * L["A1_CHUNK"]
+        assert np.all((m & 7) % 2 == 0)  # 4-byte stores stay inside their 16-byte core-matrix row
+    # stage-A epilogue: row r = ch*128 + m, 8 bins per 16 columns -> A2 rows t N1 + 8 c16 (8 rows), K n2 / N2 + n2
+    for chn in range(L["CHA"]):
+        mm = np.arange(128)
+        rr = chn * 128 + mm
+        tt, nn2 = rr // N2, rr % N2
+        for c16 in range(KA // 16):
+            r2 = tt * N1 + c16 * 8
+            cb, m2 = r2 >> 7, r2 & 127
+            assert cb.max() < L["CHB"] and np.all(m2 % 8 == 0)
+            for k in (nn2, N2 + nn2):
+                off = cb * L["A2_CHUNK"] + umma_offset_mn(m2, k, L["SBO_B"])
+                assert (off + 16).max() <= L["CHB"] * L["A2_CHUNK"]
+            assert (c16 * 8 + 7) * (N2 - 1) < n  # twiddle index k1 n2
+    # MMA reads: last byte of a 128-row chunk, and of the DFT matrices
+    assert umma_offset_mn(127, KA - 1, L["SBO_A"]) + 2 <= L["A1_CHUNK"]
+    assert umma_offset_mn(127, KB - 1, L["SBO_B"]) + 2 <= L["A2_CHUNK"]
+    assert umma_offset(KA - 1, KA - 1, KA) + 2 <= L["FA"]
+    assert umma_offset(KB - 1, KB - 1, KB) + 2 <= L["FB"]
+    # stage-B epilogue: rows t N1 + k1 -> output k1 + N1 k2 < n
+    assert (N1 - 1) + N1 * (N2 - 1) < n
+
+
+def tc_rows_tile(x: np.ndarray, forward: bool, fmt: int) -> np.ndarray:
+    """One tile of tc_rows_kernel: tile-max scale before stage A (FP16), fixed 2^-(log2 N1 + 1) before stage B."""
+    n = x.shape[-1]
+    N1, N2, TB = ROWS_CONFIGS[n]
+    x = np.asarray(x, np.complex64).reshape(-1, n)
+    ntr = x.shape[0]
+    xs = np.zeros((TB, n), np.complex64)
+    xs[:ntr] = x
+    s1 = range_scale(float(np.max(np.abs(np.concatenate([xs.real.ravel(), xs.imag.ravel()])))), fmt)
+    sb = 1.0 / (2 * N1) if fmt == 0 else 1.0
+    v = xs.reshape(TB, N1, N2)
+    A = np.concatenate([(v.real * np.float32(s1)).transpose(0, 2, 1),
+                        (v.imag * np.float32(s1)).transpose(0, 2, 1)], axis=2).reshape(TB * N2, 2 * N1)
+    ah, al = split(A, fmt)
+    fh, fl = dft_matrix(N1, forward, fmt)  # rows (k1, c), cols (n1, ci) interleaved
+    # reorder the matrix columns to (ci, n1) blocks, as the B operand stores them
+    perm = np.concatenate([np.arange(0, 2 * N1, 2), np.arange(1, 2 * N1, 2)])
+    fh, fl = fh[:2 * N1][:, perm], fl[:2 * N1][:, perm]
+    D = (ah @ fh.T + ah @ fl.T + al @ fh.T).astype(np.float32)  # rows (t, n2), cols (k1, c)
+    z = (D[:, 0::2] + 1j * D[:, 1::2]).reshape(TB, N2, N1)  # [t][n2][k1]
+    k1 = np.arange(N1)[None, :]
+    n2 = np.arange(N2)[:, None]
+    w = np.exp(-2j * np.pi * (k1 * n2) / n).astype(np.complex64)
+    if not forward:
+        w = np.conj(w)
+    y = (z * w[None] * np.float32(sb)).astype(np.complex64)  # [t][n2][k1]
+    B = np.concatenate([y.real.transpose(0, 2, 1), y.imag.transpose(0, 2, 1)], axis=2).reshape(TB * N1, 2 * N2)
+    bh, bl = split(B, fmt)
+    gh, gl = dft_matrix(N2, forward, fmt)
+    perm2 = np.concatenate([np.arange(0, 2 * N2, 2), np.arange(1, 2 * N2, 2)])
+    gh, gl = gh[:2 * N2][:, perm2], gl[:2 * N2][:, perm2]
+    D2 = (bh @ gh.T + bh @ gl.T + bl @ gh.T).astype(np.float32) / np.float32(s1 * sb)  # rows (t, k1), cols (k2, c)
+    X = (D2[:, 0::2] + 1j * D2[:, 1::2]).reshape(TB, N1, N2)  # [t][k1][k2] -> index k1 + N1 k2
+    return X.transpose(0, 2, 1).reshape(TB, n)[:ntr].astype(np.complex64)
+
+
+def tc_fft_rows(x: np.ndarray, forward: bool, fmt: int) -> np.ndarray:
+    n = x.shape[-1]
+    TB = ROWS_CONFIGS[n][2]
+    x = np.asarray(x).reshape(-1, n)
+    return np.concatenate([tc_rows_tile(x[i:i + TB], forward, fmt) for i in range(0, x.shape[0], TB)])
+
+
 def tc_fft(x: np.ndarray, forward: bool, fmt: int) -> np.ndarray:
     n = x.shape[-1]
     TB = CONFIGS[n][2]

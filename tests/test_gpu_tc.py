@@ -58,13 +58,38 @@ def test_c2c_rows(cuda, n, direction, precision):
     rng = np.random.default_rng(n + precision)
     x = _rand_complex(rng, (batch, n))
     y, desc = _run([n], C2C, direction, batch, x, precision)
-    assert "tensor-core" in desc, desc
+    assert "tensor-core" in desc and " rows " in desc, desc
     f = direction == FWD
     err = oracle.rel_l2(y, oracle.c2c(x, f))
     assert err <= oracle.tolerance(n), (err, desc)
     if precision == fft.PRECISION_FP16X3:
-        model = tc_model.tc_fft(x[:2 * tb + 1], f, 0)
-        assert oracle.rel_l2(y[:2 * tb + 1], model) <= 2e-6
+        rtb = tc_model.ROWS_CONFIGS[n][2]
+        model = tc_model.tc_fft_rows(x[:2 * rtb], f, 0)
+        assert oracle.rel_l2(y[:2 * rtb], model) <= 2e-6
+
+
+@pytest.mark.parametrize("precision", MODES, ids=["fp16x3", "bf16x3"])
+@pytest.mark.parametrize("n", [1024, 2048, 4096])
+def test_c2c_rows_8_byte_aligned_buffers(cuda, n, precision):
+    """Rows that start 8 bytes off a 16-byte boundary take the two-load path of the row pipeline."""
+    import torch
+
+    rows = 9
+    rng = np.random.default_rng(n)
+    x = _rand_complex(rng, (rows, n))
+    plan = fft.FftPlan([n], C2C, FWD, rows, precision=precision)
+    try:
+        flat = torch.zeros(rows * n + 1, dtype=torch.complex64, device="cuda")
+        xin = flat[1:].view(rows, n)
+        xin.copy_(torch.from_numpy(x))
+        out = torch.zeros(rows * n + 1, dtype=torch.complex64, device="cuda")[1:].view(rows, n)
+        assert xin.data_ptr() % 16 == 8
+        assert plan.exec_raw(xin.data_ptr(), out.data_ptr()) == fft.ACL_SUCCESS
+        torch.cuda.synchronize()
+        assert fft.asdFftSynchronize(plan.handle) == fft.ACL_SUCCESS
+        assert oracle.rel_l2(out.cpu().numpy(), oracle.c2c(x, True)) <= oracle.tolerance(n)
+    finally:
+        plan.close()
 
 
 @pytest.mark.parametrize("precision", MODES, ids=["fp16x3", "bf16x3"])
@@ -81,7 +106,7 @@ def test_c2c_vertical_columns(cuda, precision):
     rng = np.random.default_rng(3)
     x = _rand_complex(rng, (n, batch))
     y, desc = _run([n], C2C, FWD, batch, x, precision, fft.ASCEND_FFT_VERTICAL)
-    assert "tensor-core" in desc, desc
+    assert "tensor-core" in desc and " tile " in desc, desc
     assert oracle.rel_l2(y, oracle.c2c(x.T, True).T) <= oracle.tolerance(n)
 
 

@@ -52,6 +52,24 @@ def test_kernel_indices_in_bounds(n):
     tc_model.check_bounds(n)
 
 
+@pytest.mark.parametrize("n", sorted(tc_model.ROWS_CONFIGS))
+def test_row_pipeline_indices_in_bounds(n):
+    tc_model.check_rows_bounds(n)
+
+
+@pytest.mark.parametrize("n", sorted(tc_model.ROWS_CONFIGS))
+@pytest.mark.parametrize("fmt", [0, 1], ids=["fp16x3", "bf16x3"])
+@pytest.mark.parametrize("forward", [True, False], ids=["fwd", "inv"])
+def test_row_pipeline_model_accuracy(n, fmt, forward):
+    rng = np.random.default_rng(3 * n + fmt + int(forward))
+    TB = tc_model.ROWS_CONFIGS[n][2]
+    x = (rng.uniform(-1, 1, (2 * TB + 1, n)) + 1j * rng.uniform(-1, 1, (2 * TB + 1, n))).astype(np.complex64)
+    err = oracle.rel_l2(tc_model.tc_fft_rows(x, forward, fmt), oracle.c2c(x, forward))
+    assert err <= 1e-6 * np.log2(n), err
+    if fmt == 0:
+        assert err <= 2e-7
+
+
 @pytest.mark.parametrize("n", sorted(tc_model.CONFIGS))
 @pytest.mark.parametrize("fmt", [0, 1], ids=["fp16x3", "bf16x3"])
 @pytest.mark.parametrize("forward", [True, False], ids=["fwd", "inv"])
