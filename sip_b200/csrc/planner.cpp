@@ -248,7 +248,7 @@ struct Builder {
                 p.tables.push_back(fa);
                 p.tables.push_back(fb);
                 const int64_t tiles = (s.d.n_cols + tc.tb - 1) / tc.tb;
-                const int per_sm = std::max(1, kernel_blocks_per_sm(fn, 416, smem));
+                const int per_sm = std::max(1, kernel_blocks_per_sm(fn, kTcRowThreads, smem));
                 s.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(per_sm) * sm_count(device))));
                 s.d.tb = tc.tb;
                 s.has_row = false;

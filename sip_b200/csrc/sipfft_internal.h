@@ -70,7 +70,9 @@ void tc_kernel_fns(std::vector<const void *> &out);
 cudaError_t fill_tc_matrix(uint16_t *hi, uint16_t *lo, int N, int fmt, bool fwd, cudaStream_t st);
 cudaError_t launch_tc(const TileDesc &d, int n, int fmt, bool fwd, const uint16_t *const *mats, const float2 *tw,
                       int grid, int *err, cudaStream_t st);
-// Warp-specialised tensor-core kernel for contiguous C2C rows (tc_rows.cu).
+// Warp-specialised tensor-core kernel for contiguous C2C rows (tc_rows.cu):
+// 8 loader warps, 4 + 4 epilogue warps and one MMA warp.
+constexpr int kTcRowThreads = 544;
 bool tc_rows_config(int n, TcConfig &c);
 const void *tc_rows_kernel_fn(int n, int fmt, bool fwd, size_t *smem);
 void tc_rows_kernel_fns(std::vector<const void *> &out);

@@ -68,6 +68,12 @@ __device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t *r)
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// Prefetch [p, p + bytes) into L2 (p 16-byte aligned, bytes a multiple of 16).
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // mbarrier arrive (count 1) by the calling thread
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 {

@@ -20,11 +20,14 @@
 // before stage B, which bounds |Y| by the stage-A range, so no operand can
 // overflow; the BF16 form needs no scaling.
 //
-// Roles (416 threads, one CTA per SM, tiles of TB transforms round-robin):
-//   warps 0-3   load the tile from HBM, scale, split and store operand A1
-//   warps 4-7   read stage-A accumulators, twiddle, split, store operand A2
-//   warps 8-11  read stage-B accumulators and store the result to HBM
-//   warp 12     one thread issues the MMAs and commits them to mbarriers
+// Roles (544 threads, one CTA per SM, tiles of TB transforms round-robin):
+//   warps 0-7   load the tile from HBM into registers (and prefetch the next
+//               tile into L2), scale, split and store operand A1
+//   warps 8-15  per tile: read the stage-A accumulators, twiddle, split and
+//               store operand A2; then read the previous tile's stage-B
+//               accumulators and store that result to HBM (two warps per
+//               TMEM lane quarter, each with half of the columns)
+//   warp 16     one thread issues the MMAs and commits them to mbarriers
 // Accumulators are double-buffered in TMEM (D1[2], D2[2]); operands A1 and
 // A2 are single buffers.  Every wait is a bounded mbarrier poll that also
 // watches a CTA-wide abort flag, so a stalled tensor core ends the kernel
@@ -59,7 +62,8 @@ struct TcRowShape {
     static constexpr int OFF_A1 = OFF_FB + (N1 == N2 ? 0 : 2 * FB);
     static constexpr int OFF_A2 = OFF_A1 + 2 * CHA * A1_CHUNK;
     static constexpr int SMEM = OFF_A2 + 2 * CHB * A2_CHUNK;
-    static constexpr int THREADS = 416;
+    static constexpr int THREADS = kTcRowThreads;
+    static_assert(n % 512 == 0, "loader: 256 threads x element pairs per transform");
     static_assert(RA % 128 == 0 && RB % 128 == 0, "tile rows must fill 128-row MMA chunks");
     static_assert(CHA * KA == CHB * KB, "both accumulators have the same width");
     static_assert(DC == 64 || DC == 128, "accumulator width");
@@ -151,16 +155,25 @@ struct TcRowArgs {
 };
 
 namespace {
+// Streaming loads of the input (read once): no L1 allocation, so the
+// twiddle table the stage-A epilogue reads stays in L1.
 __device__ __forceinline__ float4 load_pair(const float2 *p, bool aligned16)
 {
-    if (aligned16) return __ldg(reinterpret_cast<const float4 *>(p));
-    const float2 u = __ldg(p), v = __ldg(p + 1);
-    return make_float4(u.x, u.y, v.x, v.y);
+    float4 r;
+    if (aligned16) {
+        asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+                     : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+                     : "l"(p));
+    } else {
+        asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(r.x), "=f"(r.y) : "l"(p));
+        asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(r.z), "=f"(r.w) : "l"(p + 1));
+    }
+    return r;
 }
 }  // namespace
 
 template <int N1, int N2, int TB, int FMT, bool FWD>
-__global__ void __launch_bounds__(416, 1) tc_rows_kernel(const __grid_constant__ TcRowArgs a)
+__global__ void __launch_bounds__(kTcRowThreads, 1) tc_rows_kernel(const __grid_constant__ TcRowArgs a)
 {
     using S = TcRowShape<N1, N2, TB>;
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -184,14 +197,14 @@ __global__ void __launch_bounds__(416, 1) tc_rows_kernel(const __grid_constant__
         }
     }
     if (tid == 0) {
-        mbar_init(&h->a1_full, 128);
-        mbar_init(&h->a2_full, 128);
-        mbar_init(&h->max_bar, 128);
+        mbar_init(&h->a1_full, 256);
+        mbar_init(&h->a2_full, 256);
+        mbar_init(&h->max_bar, 256);
         for (int b = 0; b < 2; b++) {
             mbar_init(&h->sa_done[b], 1);
             mbar_init(&h->sb_done[b], 1);
-            mbar_init(&h->d1_empty[b], 128);
-            mbar_init(&h->d2_empty[b], 128);
+            mbar_init(&h->d1_empty[b], 256);
+            mbar_init(&h->d2_empty[b], 256);
         }
         h->abort = 0;
         for (int i = 0; i < 4; i++) h->smax[i] = 0;
@@ -207,24 +220,38 @@ __global__ void __launch_bounds__(416, 1) tc_rows_kernel(const __grid_constant__
     tc_fence_after();
     const uint32_t tmem = h->tmem;
 
-    if (warp < 4) {
+    if (warp < 8) {
         // ================================================================ loader: HBM -> operand A1
+        // Thread tid owns element pairs (e, e+1), e = 2 tid + 512 j, of every
+        // transform of the tile: the whole tile sits in registers (one pass,
+        // also for the FP16 tile maximum), n2 = e mod N2 is fixed per thread.
+        constexpr int JT = S::n / 512, ITER = TB * JT;
         const float2 *in = a.in;
+        const int e0 = 2 * tid, n2 = e0 % N2, n1_0 = e0 / N2;
         int it = 0;
         for (int64_t g = blockIdx.x; g < num_tiles; g += gridDim.x, it++) {
             const int64_t row0 = g * TB;
             const int ntr = static_cast<int>(a.rows - row0 < TB ? a.rows - row0 : TB);
+            if (tid == 0 && a.aligned16) {
+                // pull this CTA's next tile into L2 while this one is processed
+                const int64_t g2 = g + gridDim.x;
+                for (int t = 0; g2 < num_tiles && t < TB && g2 * TB + t < a.rows; t++)
+                    prefetch_l2(in + (g2 * TB + t) * a.in_dist, S::n * 8);
+            }
+            float4 v[ITER];
+#pragma unroll
+            for (int j = 0; j < ITER; j++) {
+                const int t = j / JT, jj = j % JT;
+                v[j] = t < ntr ? load_pair(in + (row0 + t) * a.in_dist + e0 + 512 * jj, a.aligned16 != 0)
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
             float s1 = 1.0f;
             if constexpr (FMT == 0) {
-                // tile maximum (first pass; the second pass re-reads from L2)
                 if (tid == 0) h->smax[(it + 2) & 3] = 0;
                 float mx = 0.f;
-#pragma unroll 8
-                for (int q = tid; q < ntr * (S::n / 2); q += 128) {
-                    const int t = q / (S::n / 2), e = 2 * (q % (S::n / 2));
-                    const float4 v = load_pair(in + (row0 + t) * a.in_dist + e, a.aligned16 != 0);
-                    mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
-                }
+#pragma unroll
+                for (int j = 0; j < ITER; j++)
+                    mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v[j].x), fabsf(v[j].y)), fmaxf(fabsf(v[j].z), fabsf(v[j].w))));
                 for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
                 if (lane == 0) atomicMax(&h->smax[it & 3], __float_as_uint(mx));
                 mbar_arrive(&h->max_bar);
@@ -234,16 +261,14 @@ __global__ void __launch_bounds__(416, 1) tc_rows_kernel(const __grid_constant__
             }
             // operand A1 is free once the previous tile's stage A has completed
             if (it >= 1 && !tc_wait(&h->sa_done[(it - 1) & 1], ((it - 1) >> 1) & 1, h, a.err)) break;
-#pragma unroll 4
-            for (int q = tid; q < TB * (S::n / 2); q += 128) {
-                const int t = q / (S::n / 2), e = 2 * (q % (S::n / 2));
-                const int n1 = e / N2, n2 = e % N2;
+#pragma unroll
+            for (int j = 0; j < ITER; j++) {
+                const int t = j / JT, jj = j % JT;
+                const int n1 = n1_0 + (512 / N2) * jj;
                 const int r = t * N2 + n2, ch = r >> 7, m = r & 127;
-                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (t < ntr) v = load_pair(in + (row0 + t) * a.in_dist + e, a.aligned16 != 0);
                 uint32_t rh, rl, ih, il;
-                split2<FMT>(v.x * s1, v.z * s1, rh, rl);
-                split2<FMT>(v.y * s1, v.w * s1, ih, il);
+                split2<FMT>(v[j].x * s1, v[j].z * s1, rh, rl);
+                split2<FMT>(v[j].y * s1, v[j].w * s1, ih, il);
                 unsigned char *base = a1 + ch * S::A1_CHUNK;
                 const uint32_t o_re = umma_offset_mn(m, n1, S::SBO_A), o_im = umma_offset_mn(m, N1 + n1, S::SBO_A);
                 constexpr int LO = S::CHA * S::A1_CHUNK;
@@ -255,77 +280,35 @@ __global__ void __launch_bounds__(416, 1) tc_rows_kernel(const __grid_constant__
             fence_proxy_async_smem();
             mbar_arrive(&h->a1_full);
         }
-    } else if (warp < 8) {
-        // ================================================================ stage-A epilogue: D1 -> twiddle -> A2
-        const int m = tid - 128, quarter = warp & 3;
+    } else if (warp < 16) {
+        // ================================================================ epilogues (8 warps)
+        // Warps w and w + 4 share TMEM lane quarter w and split the columns.
+        // Per tile i: stage-A epilogue of i (D1 -> twiddle -> A2), then the
+        // stage-B epilogue of tile i - 1 (D2 -> HBM), which runs while the
+        // tensor core computes stage B of tile i.
+        const int quarter = warp & 3, half = (warp - 8) >> 2;
+        const int m = quarter * 32 + lane;
         constexpr float kScaleB = FMT == 0 ? 1.0f / float(2 << ilog2c<N1>()) : 1.0f;
-        int it = 0;
-        for (int64_t g = blockIdx.x; g < num_tiles; g += gridDim.x, it++) {
-            if (!tc_wait(&h->sa_done[it & 1], (it >> 1) & 1, h, a.err)) break;
-            // operand A2 is free once the previous tile's stage B has completed
-            if (it >= 1 && !tc_wait(&h->sb_done[(it - 1) & 1], ((it - 1) >> 1) & 1, h, a.err)) break;
-            tc_fence_after();
-            const uint32_t dcol = tmem + (uint32_t(quarter * 32) << 16) + (it & 1) * S::DC;
-#pragma unroll 1
-            for (int ch = 0; ch < S::CHA; ch++) {
-                const int r = ch * 128 + m, t = r / N2, n2 = r % N2;
-#pragma unroll 1
-                for (int c16 = 0; c16 < S::KA / 16; c16++) {
-                    uint32_t v[16];
-                    tmem_ld16_nowait(dcol + ch * S::KA + c16 * 16, v);
-                    tmem_wait_ld();
-                    float re[8], im[8];
+        // this thread's rows all have n2 = m mod N2; twiddle W^(k1 n2) for
+        // k1 = 16 c + i is W^(16 c n2) * W^(i n2), the second factor kept here
+        const int n2 = m % N2;
+        float2 bw[16];
 #pragma unroll
-                    for (int i = 0; i < 8; i++) {
-                        const int k1 = c16 * 8 + i;
-                        const float2 w = dir<FWD>(__ldg(a.tw + k1 * n2));
-                        const float2 z = cmul(make_float2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1])), w);
-                        re[i] = z.x * kScaleB;
-                        im[i] = z.y * kScaleB;
-                    }
-                    uint4 rh, rl, ih, il;
-                    split2<FMT>(re[0], re[1], rh.x, rl.x);
-                    split2<FMT>(re[2], re[3], rh.y, rl.y);
-                    split2<FMT>(re[4], re[5], rh.z, rl.z);
-                    split2<FMT>(re[6], re[7], rh.w, rl.w);
-                    split2<FMT>(im[0], im[1], ih.x, il.x);
-                    split2<FMT>(im[2], im[3], ih.y, il.y);
-                    split2<FMT>(im[4], im[5], ih.z, il.z);
-                    split2<FMT>(im[6], im[7], ih.w, il.w);
-                    const int r2 = t * N1 + c16 * 8, cb = r2 >> 7, m2 = r2 & 127;
-                    unsigned char *base = a2 + cb * S::A2_CHUNK;
-                    constexpr int LO = S::CHB * S::A2_CHUNK;
-                    const uint32_t o_re = umma_offset_mn(m2, n2, S::SBO_B), o_im = umma_offset_mn(m2, N2 + n2, S::SBO_B);
-                    *reinterpret_cast<uint4 *>(base + o_re) = rh;
-                    *reinterpret_cast<uint4 *>(base + LO + o_re) = rl;
-                    *reinterpret_cast<uint4 *>(base + o_im) = ih;
-                    *reinterpret_cast<uint4 *>(base + LO + o_im) = il;
-                }
-            }
-            tc_fence_before();
-            mbar_arrive(&h->d1_empty[it & 1]);
-            fence_proxy_async_smem();
-            mbar_arrive(&h->a2_full);
-        }
-    } else if (warp < 12) {
-        // ================================================================ stage-B epilogue: D2 -> HBM
-        const int m = tid - 256, quarter = warp & 3;
-        float2 *out = a.out;
-        int it = 0;
-        for (int64_t g = blockIdx.x; g < num_tiles; g += gridDim.x, it++) {
-            if (!tc_wait(&h->sb_done[it & 1], (it >> 1) & 1, h, a.err)) break;
-            tc_fence_after();
-            const int64_t row0 = g * TB;
+        for (int i = 0; i < 16; i++) bw[i] = __ldg(a.tw + i * n2);
+        const uint32_t lane_base = tmem + (uint32_t(quarter * 32) << 16);
+
+        auto stage_b_out = [&](int j, int64_t gj) {
+            const int64_t row0 = gj * TB;
             float inv = 1.0f;
-            if constexpr (FMT == 0) inv = float(2 << ilog2c<N1>()) / *reinterpret_cast<volatile float *>(&h->scale[it & 15]);
-            const uint32_t dcol = tmem + (uint32_t(quarter * 32) << 16) + (2 + (it & 1)) * S::DC;
+            if constexpr (FMT == 0) inv = float(2 << ilog2c<N1>()) / *reinterpret_cast<volatile float *>(&h->scale[j & 15]);
+            const uint32_t dcol = lane_base + (2 + (j & 1)) * S::DC;
 #pragma unroll 1
             for (int cb = 0; cb < S::CHB; cb++) {
                 const int r = cb * 128 + m, t = r / N1, k1 = r % N1;
                 const bool valid = row0 + t < a.rows;
-                float2 *dst = out + (row0 + t) * a.out_dist + k1;
+                float2 *dst = a.out + (row0 + t) * a.out_dist + k1;
 #pragma unroll 1
-                for (int c16 = 0; c16 < S::KB / 16; c16++) {
+                for (int c16 = half * (S::KB / 32); c16 < (half + 1) * (S::KB / 32); c16++) {
                     uint32_t v[16];
                     tmem_ld16_nowait(dcol + cb * S::KB + c16 * 16, v);
                     tmem_wait_ld();
@@ -333,13 +316,86 @@ __global__ void __launch_bounds__(416, 1) tc_rows_kernel(const __grid_constant__
 #pragma unroll
                         for (int i = 0; i < 8; i++) {
                             const int k2 = c16 * 8 + i;
-                            dst[N1 * k2] = make_float2(__uint_as_float(v[2 * i]) * inv, __uint_as_float(v[2 * i + 1]) * inv);
+                            dst[N1 * k2] =
+                                make_float2(__uint_as_float(v[2 * i]) * inv, __uint_as_float(v[2 * i + 1]) * inv);
                         }
                     }
                 }
             }
             tc_fence_before();
-            mbar_arrive(&h->d2_empty[it & 1]);
+            mbar_arrive(&h->d2_empty[j & 1]);
+        };
+
+        int it = 0;
+        int64_t gprev = 0;
+        bool ok = true;
+        for (int64_t g = blockIdx.x; g < num_tiles; g += gridDim.x, it++) {
+            if (!tc_wait(&h->sa_done[it & 1], (it >> 1) & 1, h, a.err)) {
+                ok = false;
+                break;
+            }
+            // operand A2 (and accumulator D2 of tile it - 1) are ready once
+            // the previous tile's stage B has completed
+            if (it >= 1 && !tc_wait(&h->sb_done[(it - 1) & 1], ((it - 1) >> 1) & 1, h, a.err)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t dcol = lane_base + (it & 1) * S::DC;
+#pragma unroll 1
+            for (int ch = 0; ch < S::CHA; ch++) {
+                const int t = (ch * 128 + m) / N2;
+#pragma unroll 1
+                for (int c32 = half * (S::KA / 64); c32 < (half + 1) * (S::KA / 64); c32++) {
+                    // 16 bins: two TMEM loads in flight
+                    uint32_t v[32];
+                    tmem_ld16_nowait(dcol + ch * S::KA + c32 * 32, v);
+                    tmem_ld16_nowait(dcol + ch * S::KA + c32 * 32 + 16, v + 16);
+                    const float2 aw = __ldg(a.tw + 16 * c32 * n2);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int hh = 0; hh < 2; hh++) {
+                        float re[8], im[8];
+#pragma unroll
+                        for (int i = 0; i < 8; i++) {
+                            const int q = hh * 8 + i;
+                            const float2 w = dir<FWD>(cmul(aw, bw[q]));
+                            const float2 z =
+                                cmul(make_float2(__uint_as_float(v[2 * q]), __uint_as_float(v[2 * q + 1])), w);
+                            re[i] = z.x * kScaleB;
+                            im[i] = z.y * kScaleB;
+                        }
+                        uint4 rh, rl, ih, il;
+                        split2<FMT>(re[0], re[1], rh.x, rl.x);
+                        split2<FMT>(re[2], re[3], rh.y, rl.y);
+                        split2<FMT>(re[4], re[5], rh.z, rl.z);
+                        split2<FMT>(re[6], re[7], rh.w, rl.w);
+                        split2<FMT>(im[0], im[1], ih.x, il.x);
+                        split2<FMT>(im[2], im[3], ih.y, il.y);
+                        split2<FMT>(im[4], im[5], ih.z, il.z);
+                        split2<FMT>(im[6], im[7], ih.w, il.w);
+                        const int r2 = t * N1 + c32 * 16 + hh * 8, cb = r2 >> 7, m2 = r2 & 127;
+                        unsigned char *base = a2 + cb * S::A2_CHUNK;
+                        constexpr int LO = S::CHB * S::A2_CHUNK;
+                        const uint32_t o_re = umma_offset_mn(m2, n2, S::SBO_B);
+                        const uint32_t o_im = umma_offset_mn(m2, N2 + n2, S::SBO_B);
+                        *reinterpret_cast<uint4 *>(base + o_re) = rh;
+                        *reinterpret_cast<uint4 *>(base + LO + o_re) = rl;
+                        *reinterpret_cast<uint4 *>(base + o_im) = ih;
+                        *reinterpret_cast<uint4 *>(base + LO + o_im) = il;
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&h->d1_empty[it & 1]);
+            fence_proxy_async_smem();
+            mbar_arrive(&h->a2_full);
+            if (it >= 1) stage_b_out(it - 1, gprev);
+            gprev = g;
+        }
+        if (ok && it >= 1 && tc_wait(&h->sb_done[(it - 1) & 1], ((it - 1) >> 1) & 1, h, a.err)) {
+            tc_fence_after();
+            stage_b_out(it - 1, gprev);
         }
     } else if (lane == 0) {
         // ================================================================ MMA issue (one thread)
@@ -349,49 +405,62 @@ __global__ void __launch_bounds__(416, 1) tc_rows_kernel(const __grid_constant__
         const uint32_t fb_hi = smem_u32(fb), fb_lo = fb_hi + S::FB;
         const uint32_t a1_hi = smem_u32(a1), a1_lo = a1_hi + S::CHA * S::A1_CHUNK;
         const uint32_t a2_hi = smem_u32(a2), a2_lo = a2_hi + S::CHB * S::A2_CHUNK;
-        auto stage_b = [&](int j) -> bool {
-            if (!tc_wait(&h->a2_full, j & 1, h, a.err)) return false;
-            if (j >= 2 && !tc_wait(&h->d2_empty[j & 1], ((j - 2) >> 1) & 1, h, a.err)) return false;
-            tc_fence_after();
-            const uint32_t d = tmem + (2 + (j & 1)) * S::DC;
-            for (int cb = 0; cb < S::CHB; cb++) {
-                const uint32_t ah[3] = {a2_hi, a2_hi, a2_lo}, bh[3] = {fb_hi, fb_lo, fb_hi};
+        // Stage A of tile na and stage B of tile nb are issued as soon as each
+        // is ready (never one queued behind the other's wait).
+        int ntiles = 0;
+        for (int64_t g = blockIdx.x; g < num_tiles; g += gridDim.x) ntiles++;
+        int na = 0, nb = 0;
+        uint32_t idle = 0;
+        while (nb < ntiles) {
+            bool progressed = false;
+            if (na < ntiles && mbar_test_wait(&h->a1_full, na & 1) &&
+                (na < 2 || mbar_test_wait(&h->d1_empty[na & 1], ((na - 2) >> 1) & 1))) {
+                tc_fence_after();
+                const uint32_t d = tmem + (na & 1) * S::DC;
+                for (int ch = 0; ch < S::CHA; ch++) {
+                    const uint32_t ah[3] = {a1_hi, a1_hi, a1_lo}, bh[3] = {fa_hi, fa_lo, fa_hi};
 #pragma unroll
-                for (int p = 0; p < 3; p++)
+                    for (int p = 0; p < 3; p++)
 #pragma unroll
-                    for (int kb = 0; kb < S::KB / 16; kb++)
-                        tc_mma_f16(d + cb * S::KB, umma_smem_desc(ah[p] + cb * S::A2_CHUNK + kb * 256, 128, S::SBO_B),
-                                   umma_smem_desc(bh[p] + kb * 256, 128, S::KB * 16), idesc_b, (p | kb) ? 1u : 0u);
+                        for (int kb = 0; kb < S::KA / 16; kb++)
+                            tc_mma_f16(d + ch * S::KA,
+                                       umma_smem_desc(ah[p] + ch * S::A1_CHUNK + kb * 256, 128, S::SBO_A),
+                                       umma_smem_desc(bh[p] + kb * 256, 128, S::KA * 16), idesc_a, (p | kb) ? 1u : 0u);
+                }
+                tc_commit(&h->sa_done[na & 1]);
+                na++;
+                progressed = true;
             }
-            tc_commit(&h->sb_done[j & 1]);
-            return true;
-        };
-        int it = 0;
-        bool ok = true;
-        for (int64_t g = blockIdx.x; g < num_tiles; g += gridDim.x, it++) {
-            if (!tc_wait(&h->a1_full, it & 1, h, a.err) ||
-                (it >= 2 && !tc_wait(&h->d1_empty[it & 1], ((it - 2) >> 1) & 1, h, a.err))) {
-                ok = false;
+            if (nb < na && mbar_test_wait(&h->a2_full, nb & 1) &&
+                (nb < 2 || mbar_test_wait(&h->d2_empty[nb & 1], ((nb - 2) >> 1) & 1))) {
+                tc_fence_after();
+                const uint32_t d = tmem + (2 + (nb & 1)) * S::DC;
+                for (int cb = 0; cb < S::CHB; cb++) {
+                    const uint32_t ah[3] = {a2_hi, a2_hi, a2_lo}, bh[3] = {fb_hi, fb_lo, fb_hi};
+#pragma unroll
+                    for (int p = 0; p < 3; p++)
+#pragma unroll
+                        for (int kb = 0; kb < S::KB / 16; kb++)
+                            tc_mma_f16(d + cb * S::KB,
+                                       umma_smem_desc(ah[p] + cb * S::A2_CHUNK + kb * 256, 128, S::SBO_B),
+                                       umma_smem_desc(bh[p] + kb * 256, 128, S::KB * 16), idesc_b, (p | kb) ? 1u : 0u);
+                }
+                tc_commit(&h->sb_done[nb & 1]);
+                nb++;
+                progressed = true;
+            }
+            if (progressed) {
+                idle = 0;
+                continue;
+            }
+            if (*reinterpret_cast<volatile int *>(&h->abort)) break;
+            if (++idle >= kMbarPollLimit) {  // nothing became ready for about a second
+                *reinterpret_cast<volatile int *>(&h->abort) = 1;
+                atomicExch(a.err, 3);
                 break;
             }
-            tc_fence_after();
-            const uint32_t d = tmem + (it & 1) * S::DC;
-            for (int ch = 0; ch < S::CHA; ch++) {
-                const uint32_t ah[3] = {a1_hi, a1_hi, a1_lo}, bh[3] = {fa_hi, fa_lo, fa_hi};
-#pragma unroll
-                for (int p = 0; p < 3; p++)
-#pragma unroll
-                    for (int kb = 0; kb < S::KA / 16; kb++)
-                        tc_mma_f16(d + ch * S::KA, umma_smem_desc(ah[p] + ch * S::A1_CHUNK + kb * 256, 128, S::SBO_A),
-                                   umma_smem_desc(bh[p] + kb * 256, 128, S::KA * 16), idesc_a, (p | kb) ? 1u : 0u);
-            }
-            tc_commit(&h->sa_done[it & 1]);
-            if (it >= 1 && !stage_b(it - 1)) {
-                ok = false;
-                break;
-            }
+            if (idle > 64) __nanosleep(32);
         }
-        if (ok && it >= 1) stage_b(it - 1);
     }
     // every role has left its loop: on the normal path all MMAs were waited on
     // (the last stage-B commit), on an abort nothing is waited for any more
@@ -492,7 +561,7 @@ cudaError_t launch_tc_rows(int n, int fmt, bool fwd, const float2 *in, float2 *o
     const bool aligned16 = (reinterpret_cast<uintptr_t>(in) & 15) == 0 && (in_dist & 1) == 0;
     TcRowArgs args{in, out, rows, in_dist, out_dist, fa, fb, tw, err, aligned16 ? 1 : 0};
     void *params[] = {&args};
-    return cudaLaunchKernel(fn, dim3(grid), dim3(416), params, smem, st);
+    return cudaLaunchKernel(fn, dim3(grid), dim3(kTcRowThreads), params, smem, st);
 }
 
 }  // namespace sipfft
