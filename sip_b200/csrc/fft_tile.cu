@@ -40,9 +40,12 @@ constexpr int maxv_for()
 
 // Gather the R inputs of each of this thread's butterflies, apply the stage
 // twiddles and run the codelet; results stay in v until after the barrier.
+// Stage twiddles come from the stage's own table when the plan has one
+// (tws[(r-1)*ns + j mod ns]: consecutive butterflies read consecutive
+// entries), else from the length-n table (tw[r*(j mod ns)*tstep]).
 template <int R, int MAXE, bool FWD>
 __device__ __forceinline__ void stage_read(float2 *v, const float2 *row, int n, int ns, int tstep, int lane, int tpt,
-                                           bool active, const float2 *__restrict__ tw)
+                                           bool active, const float2 *__restrict__ tw, const float2 *__restrict__ tws)
 {
     constexpr int NB = nb_for<R, MAXE>();
     const int nbf = n / R;
@@ -53,9 +56,16 @@ __device__ __forceinline__ void stage_read(float2 *v, const float2 *row, int n, 
 #pragma unroll
             for (int r = 0; r < R; r++) v[b * R + r] = row[pad(j + r * nbf)];
             if (ns > 1) {
-                const int step = (j % ns) * tstep;
+                const int k = j % ns;
+                if (tws) {
 #pragma unroll
-                for (int r = 1; r < R; r++) v[b * R + r] = cmul(v[b * R + r], dir<FWD>(__ldg(tw + r * step)));
+                    for (int r = 1; r < R; r++)
+                        v[b * R + r] = cmul(v[b * R + r], dir<FWD>(__ldg(tws + (r - 1) * ns + k)));
+                } else {
+                    const int step = k * tstep;
+#pragma unroll
+                    for (int r = 1; r < R; r++) v[b * R + r] = cmul(v[b * R + r], dir<FWD>(__ldg(tw + r * step)));
+                }
             }
             dft<R, FWD>(v + b * R);
         }
@@ -89,12 +99,15 @@ template <int MAXE, bool FWD>
 __device__ __forceinline__ void run_stages(float2 *row, const TileDesc &d, int lane, bool active)
 {
     float2 v[maxv_for<MAXE>()];
+    int64_t toff = 0;  // offset of this stage's table in d.stw (stage 0 has none)
 #pragma unroll 1
     for (int s = 0; s < d.nstages; s++) {
         const int ns = d.ns[s], ts = d.tstep[s], R = d.radix[s];
+        const float2 *tws = d.stw ? d.stw + toff : nullptr;
+        if (s > 0) toff += int64_t(R - 1) * ns;
         switch (R) {
 #define SIPFFT_READ(RR) \
-    case RR: stage_read<RR, MAXE, FWD>(v, row, d.n, ns, ts, lane, d.tpt, active, d.tw); break;
+    case RR: stage_read<RR, MAXE, FWD>(v, row, d.n, ns, ts, lane, d.tpt, active, d.tw, tws); break;
             SIPFFT_RADIX_CASES(SIPFFT_READ)
 #undef SIPFFT_READ
             default: break;  // the planner only emits the radices above

@@ -89,6 +89,15 @@ bool choose_cfg(int n, bool column, int64_t ncols, TileCfg &c, std::string &err,
         err = "transform does not fit in shared memory";
         return false;
     }
+    if (column && c.tb >= 2) {
+        // column tiles: lane l = tid mod tb works on transform l, so a half warp
+        // touches tb transforms x 16/tb consecutive elements; a pitch with
+        // P mod (32/tb) = 16/tb puts them on 16 distinct 8-byte bank pairs
+        const int m = 32 / c.tb, want = 16 / c.tb;
+        int p = padded(n - 1) + 1;
+        while (p % m != want) p++;
+        if (int64_t(c.tb) * p * 8 <= kMaxSmemBytes) c.pitch = p;
+    }
     return true;
 }
 
@@ -217,6 +226,13 @@ struct Builder {
         d.out_a = oa;
         d.tw = tw;
         d.tw_mul = tw_mul;
+        if (d.nstages > 1) {
+            // contiguous per-stage twiddles: coalesced reads in every stage
+            TablePtr st = get_stage_table(d.radix, d.nstages, device, &err);
+            if (!st) return false;
+            p.tables.push_back(st);
+            d.stw = st->ptr;
+        }
         s.grid = grid_for(d.num_tiles);
         if (!column && n_outer == 1 && ia.estride == 1 && oa.estride == 1 &&
             (io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))

@@ -57,21 +57,26 @@ TablePtr get_table(int64_t count, int64_t denom, int64_t mult, int device, std::
 
 TablePtr get_stage_table(const StaticKernel &k, int device, std::string *err)
 {
+    return get_stage_table(k.radix, k.nstages, device, err);
+}
+
+TablePtr get_stage_table(const int *radix, int nstages, int device, std::string *err)
+{
     static std::mutex mu;
     static std::map<std::pair<int, std::string>, std::weak_ptr<DeviceTable>> cache;  // (device, radix sequence)
     std::lock_guard<std::mutex> lock(mu);
     std::string seq;
-    for (int s = 0; s < k.nstages; s++) seq += std::to_string(k.radix[s]) + ",";
+    for (int s = 0; s < nstages; s++) seq += std::to_string(radix[s]) + ",";
     auto key = std::make_pair(device, seq);
     auto it = cache.find(key);
     if (it != cache.end()) {
         if (TablePtr t = it->second.lock()) return t;
     }
     auto t = std::make_shared<DeviceTable>();
-    t->count = std::max<int64_t>(1, stage_twiddle_count(k.radix, k.nstages));
+    t->count = std::max<int64_t>(1, stage_twiddle_count(radix, nstages));
     t->device = device;
     cudaError_t e = cudaMalloc(&t->ptr, sizeof(float2) * static_cast<size_t>(t->count));
-    if (e == cudaSuccess) e = fill_stage_twiddles(t->ptr, k.radix, k.nstages, 0);
+    if (e == cudaSuccess) e = fill_stage_twiddles(t->ptr, radix, nstages, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
         if (err) *err = std::string("twiddle table: ") + cudaGetErrorString(e);

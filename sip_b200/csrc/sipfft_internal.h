@@ -108,6 +108,9 @@ using TablePtr = std::shared_ptr<DeviceTable>;
 TablePtr get_table(int64_t count, int64_t denom, int64_t mult, int device, std::string *err);
 // per-stage twiddle tables of a static kernel's radix sequence
 TablePtr get_stage_table(const StaticKernel &k, int device, std::string *err);
+// per-stage twiddle tables of any radix sequence: stage s >= 1 holds
+// W_{ns R}^{r k} at [(r-1) ns + k], stages back to back (stage 0 has none)
+TablePtr get_stage_table(const int *radix, int nstages, int device, std::string *err);
 // hi/lo operand matrices of one tensor-core stage (N points, fmt, direction).
 // layout 0 (A operand of tc_fft_kernel): hi at ptr, lo at ptr + 64 N float2,
 // each 128 x 2N 16-bit values; layout 1 (B operand of tc_rows_kernel): hi at

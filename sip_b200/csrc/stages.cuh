@@ -45,7 +45,8 @@ struct SmemRow {
 
 template <int R, int MAXE, bool FWD, class Src>
 __device__ __forceinline__ void stage_gather(float2 *v, const Src &src, int n, int ns, int tstep, int lane, int tpt,
-                                             bool active, const float2 *__restrict__ tw)
+                                             bool active, const float2 *__restrict__ tw,
+                                             const float2 *__restrict__ tws = nullptr)
 {
     constexpr int NB = nb_for<R, MAXE>();
     const int nbf = n / R;
@@ -62,9 +63,17 @@ __device__ __forceinline__ void stage_gather(float2 *v, const Src &src, int n, i
         const int j = lane + b * tpt;
         if (active && j < nbf) {
             if (ns > 1) {
-                const int step = (j % ns) * tstep;
+                // the stage's own table when present: consecutive butterflies, consecutive entries
+                const int k = j % ns;
+                if (tws) {
 #pragma unroll
-                for (int r = 1; r < R; r++) v[b * R + r] = cmul(v[b * R + r], dir<FWD>(__ldg(tw + r * step)));
+                    for (int r = 1; r < R; r++)
+                        v[b * R + r] = cmul(v[b * R + r], dir<FWD>(__ldg(tws + (r - 1) * ns + k)));
+                } else {
+                    const int step = k * tstep;
+#pragma unroll
+                    for (int r = 1; r < R; r++) v[b * R + r] = cmul(v[b * R + r], dir<FWD>(__ldg(tw + r * step)));
+                }
             }
             dft<R, FWD>(v + b * R);
         }
@@ -93,11 +102,11 @@ __device__ __forceinline__ void stage_scatter(const float2 *v, const Dst &dst, i
 
 template <int MAXE, bool FWD, class Src>
 __device__ __forceinline__ void gather_any(int R, float2 *v, const Src &src, int n, int ns, int ts, int lane, int tpt,
-                                           bool active, const float2 *tw)
+                                           bool active, const float2 *tw, const float2 *tws)
 {
     switch (R) {
 #define SIPFFT_G(RR) \
-    case RR: stage_gather<RR, MAXE, FWD>(v, src, n, ns, ts, lane, tpt, active, tw); break;
+    case RR: stage_gather<RR, MAXE, FWD>(v, src, n, ns, ts, lane, tpt, active, tw, tws); break;
         SIPFFT_RADIX_CASES(SIPFFT_G)
 #undef SIPFFT_G
         default: break;
@@ -135,8 +144,10 @@ __device__ __forceinline__ void run_fft(const TileDesc &d, float2 *work, const S
         if (active && lane == 0) dstL(0, src0(0));
         return;
     }
-    // stage 0
-    gather_any<MAXE, FWD>(d.radix[0], v, src0, n, d.ns[0], d.tstep[0], lane, d.tpt, active, d.tw);
+    // stage 0 (no twiddles); stage s >= 1 reads d.stw + toff when the plan has stage tables
+    int64_t toff = 0;
+    auto tws = [&](int s) -> const float2 * { return d.stw ? d.stw + toff : nullptr; };
+    gather_any<MAXE, FWD>(d.radix[0], v, src0, n, d.ns[0], d.tstep[0], lane, d.tpt, active, d.tw, nullptr);
     if (src0_in_place || (S == 1 && dstL_in_place)) __syncthreads();
     if (S == 1) {
         scatter_any<MAXE>(d.radix[0], v, dstL, n, d.ns[0], lane, d.tpt, active);
@@ -146,12 +157,14 @@ __device__ __forceinline__ void run_fft(const TileDesc &d, float2 *work, const S
     __syncthreads();
 #pragma unroll 1
     for (int s = 1; s < S - 1; s++) {
-        gather_any<MAXE, FWD>(d.radix[s], v, w, n, d.ns[s], d.tstep[s], lane, d.tpt, active, d.tw);
+        gather_any<MAXE, FWD>(d.radix[s], v, w, n, d.ns[s], d.tstep[s], lane, d.tpt, active, d.tw, tws(s));
+        toff += int64_t(d.radix[s] - 1) * d.ns[s];
         __syncthreads();
         scatter_any<MAXE>(d.radix[s], v, w, n, d.ns[s], lane, d.tpt, active);
         __syncthreads();
     }
-    gather_any<MAXE, FWD>(d.radix[S - 1], v, w, n, d.ns[S - 1], d.tstep[S - 1], lane, d.tpt, active, d.tw);
+    gather_any<MAXE, FWD>(d.radix[S - 1], v, w, n, d.ns[S - 1], d.tstep[S - 1], lane, d.tpt, active, d.tw,
+                          tws(S - 1));
     if (dstL_in_place) __syncthreads();
     scatter_any<MAXE>(d.radix[S - 1], v, dstL, n, d.ns[S - 1], lane, d.tpt, active);
 }
