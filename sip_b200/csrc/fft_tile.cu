@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "async_copy.cuh"
 #include "codelets.cuh"
 #include "fft_tile.cuh"
 #include "sipfft_internal.h"
@@ -45,7 +46,8 @@ constexpr int maxv_for()
 // entries), else from the length-n table (tw[r*(j mod ns)*tstep]).
 template <int R, int MAXE, bool FWD>
 __device__ __forceinline__ void stage_read(float2 *v, const float2 *row, int n, int ns, int tstep, int lane, int tpt,
-                                           bool active, const float2 *__restrict__ tw, const float2 *__restrict__ tws)
+                                           bool active, const float2 *__restrict__ tw, const float2 *__restrict__ tws,
+                                           const TileDesc &d, int64_t kc)
 {
     constexpr int NB = nb_for<R, MAXE>();
     const int nbf = n / R;
@@ -55,6 +57,11 @@ __device__ __forceinline__ void stage_read(float2 *v, const float2 *row, int n, 
         if (active && j < nbf) {
 #pragma unroll
             for (int r = 0; r < R; r++) v[b * R + r] = row[pad(j + r * nbf)];
+            if (kc >= 0) {
+                // inter-pass twiddle of a multi-pass step, applied on the first read
+#pragma unroll
+                for (int r = 0; r < R; r++) v[b * R + r] = cmul(v[b * R + r], pass_twiddle<FWD>(d, j + r * nbf, kc));
+            }
             if (ns > 1) {
                 const int k = j % ns;
                 if (tws) {
@@ -95,8 +102,9 @@ __device__ __forceinline__ void stage_write(const float2 *v, float2 *row, int n,
 
 // One register array is shared by all radices so that only one set of
 // butterfly values is live across each stage barrier.
+// kc >= 0: the tile's inter-pass twiddles (column kc) are still to be applied (first stage does it).
 template <int MAXE, bool FWD>
-__device__ __forceinline__ void run_stages(float2 *row, const TileDesc &d, int lane, bool active)
+__device__ __forceinline__ void run_stages(float2 *row, const TileDesc &d, int lane, bool active, int64_t kc = -1)
 {
     float2 v[maxv_for<MAXE>()];
     int64_t toff = 0;  // offset of this stage's table in d.stw (stage 0 has none)
@@ -107,7 +115,7 @@ __device__ __forceinline__ void run_stages(float2 *row, const TileDesc &d, int l
         if (s > 0) toff += int64_t(R - 1) * ns;
         switch (R) {
 #define SIPFFT_READ(RR) \
-    case RR: stage_read<RR, MAXE, FWD>(v, row, d.n, ns, ts, lane, d.tpt, active, d.tw, tws); break;
+    case RR: stage_read<RR, MAXE, FWD>(v, row, d.n, ns, ts, lane, d.tpt, active, d.tw, tws, d, s == 0 ? kc : -1); break;
             SIPFFT_RADIX_CASES(SIPFFT_READ)
 #undef SIPFFT_READ
             default: break;  // the planner only emits the radices above
@@ -153,6 +161,81 @@ __global__ void __launch_bounds__(512, 1) tile_fft_kernel(const __grid_constant_
 {
     extern __shared__ float2 sm[];
     for (int64_t g = blockIdx.x; g < d.num_tiles; g += gridDim.x) process_tile<MAXE, FWD>(d, d.in, d.out, g, sm);
+}
+
+// ------------------------------------------------------------------------------------ double-buffered tiles
+// Persistent variant for C2C tiles (column tiles of strided axes and of
+// multi-pass steps): while a tile runs its stages, the element copies of the
+// CTA's next tile are already in flight into the second buffer (cp.async,
+// 8 bytes per element, no registers held), so HBM latency overlaps compute.
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void issue_tile_c2c(const TileDesc &d, float2 *sm, int64_t g)
+{
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int64_t o = g / d.tiles_per_outer;
+    const int64_t c0 = (g % d.tiles_per_outer) * d.tb;
+    const int64_t left = d.n_cols - c0;
+    const int ntr = left < d.tb ? static_cast<int>(left) : d.tb;
+    int l, e0, estep;
+    if (d.in_a.estride == 1) {
+        l = tid / d.tpt;
+        e0 = tid % d.tpt;
+        estep = d.tpt;
+    } else {
+        l = tid % d.tb;
+        e0 = tid / d.tb;
+        estep = bd / d.tb;
+    }
+    if (l >= ntr) return;
+    const float2 *x = static_cast<const float2 *>(d.in) + col_base(d.in_a, o, c0 + l);
+    const int64_t es = d.in_a.estride;
+    float2 *row = sm + l * d.pitch;
+    for (int e = e0; e < d.n; e += estep) cp_async8(row + pad(e), x + e * es);
+}
+
+template <int MAXE, bool FWD>
+__global__ void __launch_bounds__(512, 1) tile_db_kernel(const __grid_constant__ TileDesc d)
+{
+    extern __shared__ float2 sm[];
+    const int64_t span = int64_t(d.tb) * d.pitch;
+    const int tid = threadIdx.x;
+    int l, lane;
+    if (d.xfast) {
+        l = tid % d.tb;
+        lane = tid / d.tb;
+    } else {
+        l = tid / d.tpt;
+        lane = tid % d.tpt;
+    }
+    const bool thread_on = tid < d.tb * d.tpt;
+    int64_t g = blockIdx.x;
+    if (g < d.num_tiles) issue_tile_c2c(d, sm, g);
+    cp_async_commit();
+    for (int i = 0; g < d.num_tiles; g += gridDim.x, i++) {
+        float2 *cur = sm + (i & 1) * span;
+        const int64_t gn = g + gridDim.x;
+        // the other buffer was released by the barrier that ended the previous tile
+        if (gn < d.num_tiles) issue_tile_c2c(d, sm + ((i + 1) & 1) * span, gn);
+        cp_async_commit();
+        cp_async_wait<1>();  // this tile's copies (all groups but the newest) have landed
+        __syncthreads();
+        const int64_t o = g / d.tiles_per_outer;
+        const int64_t c0 = (g % d.tiles_per_outer) * d.tb;
+        const int64_t left = d.n_cols - c0;
+        const int ntr = left < d.tb ? static_cast<int>(left) : d.tb;
+        const int64_t kc = d.g_twiddle ? (c0 + (thread_on ? l : 0)) % d.g_ns : -1;
+        run_stages<MAXE, FWD>(cur + (thread_on ? l : 0) * d.pitch, d, lane, thread_on && l < ntr, kc);
+        store_tile<FWD>(d, d.out, cur, o, c0, ntr);
+        __syncthreads();
+    }
+    cp_async_wait<0>();
 }
 
 // ------------------------------------------------------------------------------------ uneven batches
@@ -303,6 +386,29 @@ void tile_kernel_fns(std::vector<const void *> &out)
     out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<32, true>));
     out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<32, false>));
     out.push_back(reinterpret_cast<const void *>(batch_fft_kernel<32>));
+    for (int maxe : {8, 16, 32})
+        for (int f = 0; f < 2; f++) out.push_back(tile_db_kernel_fn(maxe, f != 0));
+}
+
+const void *tile_db_kernel_fn(int maxe, bool forward)
+{
+    if (maxe <= 8) return forward ? reinterpret_cast<const void *>(tile_db_kernel<8, true>)
+                                  : reinterpret_cast<const void *>(tile_db_kernel<8, false>);
+    if (maxe <= 16) return forward ? reinterpret_cast<const void *>(tile_db_kernel<16, true>)
+                                   : reinterpret_cast<const void *>(tile_db_kernel<16, false>);
+    return forward ? reinterpret_cast<const void *>(tile_db_kernel<32, true>)
+                   : reinterpret_cast<const void *>(tile_db_kernel<32, false>);
+}
+
+cudaError_t launch_tile_db(const TileDesc &d, int maxe, bool forward, int grid, cudaStream_t st)
+{
+    const int block = d.tb * d.tpt;
+    const size_t smem = 2 * static_cast<size_t>(d.tb) * d.pitch * sizeof(float2);
+    if (block <= 0 || block > 512 || smem > static_cast<size_t>(kMaxSmemBytes) || grid <= 0 || d.io != IO_C2C)
+        return cudaErrorInvalidConfiguration;
+    TileDesc dd = d;
+    void *args[] = {&dd};
+    return cudaLaunchKernel(tile_db_kernel_fn(maxe, forward), dim3(grid), dim3(block), args, smem, st);
 }
 
 cudaError_t launch_tile(const TileDesc &d, int maxe, bool forward, int grid, cudaStream_t st)

@@ -237,6 +237,15 @@ struct Builder {
         if (!column && n_outer == 1 && ia.estride == 1 && oa.estride == 1 &&
             (io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
             add_row_variant(s, c, ia.cstride, oa.cstride);
+        if (column && io == IO_C2C && 2 * int64_t(d.tb) * d.pitch * 8 <= kMaxSmemBytes) {
+            // strided C2C axis or multi-pass step: double-buffered persistent tiles
+            const size_t smem = 2 * size_t(d.tb) * d.pitch * 8;
+            const int per_sm = kernel_blocks_per_sm(tile_db_kernel_fn(s.maxe, s.forward), d.tb * d.tpt, smem);
+            if (per_sm > 0) {
+                s.db = true;
+                s.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(d.num_tiles, int64_t(per_sm) * sm_count(device))));
+            }
+        }
         if (p.precision != 0 && (io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
             return add_tc_variant(s);
         return true;
@@ -752,7 +761,7 @@ std::string describe_plan(const Plan &p)
     for (const Step &s : p.steps) {
         o << "  [" << static_cast<int>(s.src) << "->" << static_cast<int>(s.dst) << "] " << s.what;
         if (s.kind == StepKind::kTile) {
-            o << " n=" << s.d.n << " radices=";
+            o << (s.db ? " [double-buffered]" : "") << " n=" << s.d.n << " radices=";
             for (int i = 0; i < s.d.nstages; i++) o << (i ? "x" : "") << s.d.radix[i];
             o << " tb=" << s.d.tb << " tpt=" << s.d.tpt << " tiles=" << s.d.num_tiles << " grid=" << s.grid
               << " smem=" << s.d.tb * s.d.pitch * 8;

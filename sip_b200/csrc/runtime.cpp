@@ -257,6 +257,11 @@ cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const v
                                              st);
                     else
                         e = launch_row_tiles(d, s.maxe, s.forward, s.row_grid, device_error_word(p.device), st);
+                } else if (s.db) {
+                    TileDesc d = s.d;
+                    d.in = src;
+                    d.out = dst;
+                    e = launch_tile_db(d, s.maxe, s.forward, s.grid, st);
                 } else {
                     TileDesc d = s.d;
                     d.in = src;

@@ -19,6 +19,9 @@ constexpr int kMaxSmemBytes = 227 * 1024;
 constexpr int kB200Sms = 148;
 
 cudaError_t launch_tile(const TileDesc &d, int maxe, bool forward, int grid, cudaStream_t st);
+// Persistent double-buffered C2C tile kernel (cp.async prefetch of the next tile).
+const void *tile_db_kernel_fn(int maxe, bool forward);
+cudaError_t launch_tile_db(const TileDesc &d, int maxe, bool forward, int grid, cudaStream_t st);
 cudaError_t fill_twiddles(float2 *t, int64_t count, int64_t denom, int64_t mult, cudaStream_t st);
 cudaError_t fill_chirp(float2 *t, int64_t n_len, bool forward, cudaStream_t st);
 cudaError_t fill_bluestein_b(float2 *b, const float2 *chirp, int64_t n_len, int64_t m_len, cudaStream_t st);
@@ -132,6 +135,7 @@ struct Step {
     // optional TMA-pipelined row variant of the same step (used when the
     // source pointer is 16-byte aligned); row_fn != nullptr selects a
     // compile-time specialised kernel instead of the runtime-radix one
+    bool db = false;  // run d on the double-buffered tile kernel (grid is then persistent)
     bool has_row = false;
     TileDesc rd{};
     int row_grid = 1;
