@@ -273,7 +273,7 @@ struct BatchPlan {
     int2 *d_items = nullptr;
     int *d_counters = nullptr;  // [0] = item counter, [1 + s] = tiles done of segment s
     size_t ws_bytes = 0;
-    int grid = 1, block = 512;
+    int grid = 1, block = kBatchBlock;
     size_t smem = 0;
     std::vector<TablePtr> tables;
     int64_t in_elems = 0, out_elems = 0;
@@ -318,8 +318,12 @@ std::string build_batch(BatchPlan &bp)
         p.batch = b;
         p.device = bp.device;
         p.use_tuned = true;
-        p.row_threads = 512;
-        p.row_smem = 160 * 1024;  // leaves room for the kernel's static shared memory
+        // tiles of at most 256 threads x 16 points and a few tens of KB, so that
+        // several CTAs of the one batch kernel share an SM: longer rows go multi-pass
+        p.row_threads = 256;
+        p.row_smem = 48 * 1024;
+        p.max_row_n = kBatchMaxRowN;
+        p.max_maxe = kBatchMaxe;
         std::string e = build_plan_1d(p);
         if (!e.empty()) return "length " + std::to_string(n) + ": " + e;
         const size_t ws0 = (p.ws_buf_bytes[0] + 255) / 256 * 256;
@@ -345,7 +349,9 @@ std::string build_batch(BatchPlan &bp)
             sg.ntiles = static_cast<int>(s.d.num_tiles);
             sg.fwd = s.forward ? 1 : 0;
             if (s.d.tb * s.d.tpt > bp.block) return "tile shape exceeds the batch block size";
-            bp.smem = std::max(bp.smem, static_cast<size_t>(s.d.tb) * s.d.pitch * sizeof(float2));
+            if (s.maxe > kBatchMaxe) return "tile needs more points per thread than the batch kernel holds";
+            // two buffers per CTA (the batch kernel prefetches its next item)
+            bp.smem = std::max(bp.smem, 2 * static_cast<size_t>(s.d.tb) * s.d.pitch * sizeof(float2));
             const int phase = p.steps.size() == 1 ? 1 : (i == 0 ? 0 : static_cast<int>(i) + 1);
             order.push_back({static_cast<int>(bp.segs.size()), phase, double(s.d.n) * s.d.tb});
             bp.segs.push_back(sg);
@@ -365,7 +371,7 @@ std::string build_batch(BatchPlan &bp)
     for (const Pending &pd : order)
         for (int t = 0; t < bp.segs[pd.seg].ntiles; t++) bp.items.push_back(make_int2(pd.seg, t));
     if (bp.items.size() > 0x7fffffff) return "too many tiles";
-    const int per_sm = kernel_blocks_per_sm(batch_kernel_fn(), bp.block, bp.smem);
+    const int per_sm = kernel_blocks_per_sm(batch_kernel_fn(bp.forward), bp.block, bp.smem);
     if (per_sm <= 0) return "batch kernel does not fit on an SM";
     bp.grid = per_sm * sm_count(bp.device);
     size_t bytes = bp.segs.size() * sizeof(BatchSeg);
@@ -387,7 +393,7 @@ cudaError_t enqueue(BatchPlan &bp, const void *in, void *out, void *ws, cudaStre
     if (e != cudaSuccess) return e;
     BatchBufs bufs{{const_cast<void *>(in), out, ws, nullptr}};
     return launch_batch(bp.grid, bp.block, bp.smem, bp.d_segs, bp.d_items, static_cast<int>(bp.items.size()),
-                        bp.d_counters, bp.d_counters + 1, bufs, device_error_word(bp.device), st);
+                        bp.d_counters, bp.d_counters + 1, bufs, device_error_word(bp.device), bp.forward, st);
 }
 
 std::mutex g_batch_mu;

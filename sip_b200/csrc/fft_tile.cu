@@ -132,8 +132,21 @@ __device__ __forceinline__ void run_stages(float2 *row, const TileDesc &d, int l
     }
 }
 
+__device__ __forceinline__ void conj_tile(const TileDesc &d, float2 *sm, int ntr)
+{
+    for (int i = threadIdx.x; i < ntr * d.n; i += blockDim.x) {
+        float2 *p = sm + (i / d.n) * d.pitch + pad(i % d.n);
+        p->y = -p->y;
+    }
+}
+
+// flip: the segment's direction is the opposite of FWD (C2C / Bluestein tiles only:
+// their load and store phases do not depend on the direction)
+// loaded: the tile's input already sits in sm (copied by cp.async, inter-pass
+// twiddles not applied yet)
 template <int MAXE, bool FWD>
-__device__ __forceinline__ void process_tile(const TileDesc &d, const void *in, void *out, int64_t g, float2 *sm)
+__device__ __forceinline__ void process_tile(const TileDesc &d, const void *in, void *out, int64_t g, float2 *sm,
+                                             bool flip = false, bool loaded = false)
 {
     const int tid = threadIdx.x;
     int l, lane;
@@ -149,9 +162,20 @@ __device__ __forceinline__ void process_tile(const TileDesc &d, const void *in, 
     const int64_t c0 = (g % d.tiles_per_outer) * d.tb;
     const int64_t left = d.n_cols - c0;
     const int ntr = left < d.tb ? static_cast<int>(left) : d.tb;
-    load_tile<FWD>(d, in, sm, o, c0, ntr);
-    __syncthreads();
-    run_stages<MAXE, FWD>(sm + (thread_on ? l : 0) * d.pitch, d, lane, thread_on && l < ntr);
+    if (!loaded) {
+        load_tile<FWD>(d, in, sm, o, c0, ntr);
+        __syncthreads();
+    }
+    const int64_t kc = loaded && d.g_twiddle ? (c0 + (thread_on ? l : 0)) % d.g_ns : -1;
+    if (flip) {
+        conj_tile(d, sm, ntr);
+        __syncthreads();
+    }
+    run_stages<MAXE, FWD>(sm + (thread_on ? l : 0) * d.pitch, d, lane, thread_on && l < ntr, kc);
+    if (flip) {
+        conj_tile(d, sm, ntr);
+        __syncthreads();
+    }
     store_tile<FWD>(d, out, sm, o, c0, ntr);
     __syncthreads();
 }
@@ -176,7 +200,7 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-__device__ __forceinline__ void issue_tile_c2c(const TileDesc &d, float2 *sm, int64_t g)
+__device__ __forceinline__ void issue_tile_c2c(const TileDesc &d, const void *in, float2 *sm, int64_t g)
 {
     const int tid = threadIdx.x, bd = blockDim.x;
     const int64_t o = g / d.tiles_per_outer;
@@ -194,7 +218,7 @@ __device__ __forceinline__ void issue_tile_c2c(const TileDesc &d, float2 *sm, in
         estep = bd / d.tb;
     }
     if (l >= ntr) return;
-    const float2 *x = static_cast<const float2 *>(d.in) + col_base(d.in_a, o, c0 + l);
+    const float2 *x = static_cast<const float2 *>(in) + col_base(d.in_a, o, c0 + l);
     const int64_t es = d.in_a.estride;
     float2 *row = sm + l * d.pitch;
     for (int e = e0; e < d.n; e += estep) cp_async8(row + pad(e), x + e * es);
@@ -216,13 +240,13 @@ __global__ void __launch_bounds__(512, 1) tile_db_kernel(const __grid_constant__
     }
     const bool thread_on = tid < d.tb * d.tpt;
     int64_t g = blockIdx.x;
-    if (g < d.num_tiles) issue_tile_c2c(d, sm, g);
+    if (g < d.num_tiles) issue_tile_c2c(d, d.in, sm, g);
     cp_async_commit();
     for (int i = 0; g < d.num_tiles; g += gridDim.x, i++) {
         float2 *cur = sm + (i & 1) * span;
         const int64_t gn = g + gridDim.x;
         // the other buffer was released by the barrier that ended the previous tile
-        if (gn < d.num_tiles) issue_tile_c2c(d, sm + ((i + 1) & 1) * span, gn);
+        if (gn < d.num_tiles) issue_tile_c2c(d, d.in, sm + ((i + 1) & 1) * span, gn);
         cp_async_commit();
         cp_async_wait<1>();  // this tile's copies (all groups but the newest) have landed
         __syncthreads();
@@ -245,54 +269,107 @@ __global__ void __launch_bounds__(512, 1) tile_db_kernel(const __grid_constant__
 // multi-pass transform, the second half of a Bluestein transform) waits,
 // with a bounded spin, until every tile of that segment has been published.
 // Items are ordered so that every producer tile is dequeued before its
-// consumers and all CTAs are resident (grid = occupancy), so the waits end.
-template <int MAXE>
-__global__ void __launch_bounds__(512, 1)
+// consumers and all CTAs are resident (grid = occupancy), so the waits end:
+// a CTA holds at most two items (the one it computes and the next one it
+// prefetches) and each waits only on items dequeued before it.
+//
+// Double buffering: while an item computes in one shared-memory buffer, the
+// CTA dequeues its next item and, when that is a plain C2C tile whose
+// producer has already finished, starts its element copies (cp.async) into
+// the other buffer.  Other items (Bluestein halves, producers still running)
+// load synchronously when their turn comes.
+__device__ __forceinline__ bool batch_dep_done(const BatchSeg *segs, int *done, const BatchSeg &sg)
+{
+    if (sg.dep < 0) return true;
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(done + sg.dep) : "memory");
+    return v >= segs[sg.dep].ntiles;
+}
+
+__device__ __forceinline__ bool batch_dep_wait(const BatchSeg *segs, int *done, const BatchSeg &sg, int *err)
+{
+    for (uint32_t poll = 0; poll < (1u << 24); poll++) {
+        if (batch_dep_done(segs, done, sg)) return true;
+        __nanosleep(128);
+    }
+    atomicExch(err, 2);
+    return false;
+}
+
+template <int MAXE, bool FWD>
+__global__ void __launch_bounds__(kBatchBlock, 2)
     batch_fft_kernel(const BatchSeg *__restrict__ segs, const int2 *__restrict__ items, int nitems, int *counter,
-                     int *done, BatchBufs bufs, int *err)
+                     int *done, BatchBufs bufs, int *err, int64_t span)
 {
     extern __shared__ float2 sm[];
-    __shared__ int s_item;
-    __shared__ int s_ok;
+    __shared__ int s_item, s_pref, s_ok;
     const int tid = threadIdx.x;
-    for (;;) {
-        if (tid == 0) s_item = atomicAdd(counter, 1);
-        __syncthreads();
-        const int w = s_item;
-        __syncthreads();
-        if (w >= nitems) break;
-        const int2 it = items[w];
-        const BatchSeg &sg = segs[it.x];
-        if (sg.dep >= 0) {
-            if (tid == 0) {
-                const int need = segs[sg.dep].ntiles;
-                int ok = 0;
-                for (uint32_t poll = 0; poll < (1u << 24); poll++) {
-                    int v;
-                    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(done + sg.dep) : "memory");
-                    if (v >= need) {
-                        ok = 1;
-                        break;
-                    }
-                    __nanosleep(128);
-                }
-                if (!ok) atomicExch(err, 2);
-                s_ok = ok;
-            }
-            __syncthreads();
-            if (!s_ok) continue;  // give up on this item; the error word reports it
-        }
-        const char *in = static_cast<const char *>(bufs.p[sg.in_buf]) + sg.in_off;
-        char *out = static_cast<char *>(bufs.p[sg.out_buf]) + sg.out_off;
-        if (sg.fwd)
-            process_tile<MAXE, true>(sg.d, in, out, it.y, sm);
-        else
-            process_tile<MAXE, false>(sg.d, in, out, it.y, sm);
-        if (tid == 0) {
-            __threadfence();
-            atomicAdd(done + it.x, 1);
+    // dequeue the first item; prefetch it when it is ready to read
+    if (tid == 0) {
+        s_item = atomicAdd(counter, 1);
+        s_pref = 0;
+        if (s_item < nitems) {
+            const BatchSeg &sg = segs[items[s_item].x];
+            s_pref = sg.d.io == IO_C2C && batch_dep_done(segs, done, sg);
         }
     }
+    __syncthreads();
+    int w = s_item;
+    bool pref = s_pref != 0;
+    if (w < nitems && pref) {
+        const int2 it = items[w];
+        const BatchSeg &sg = segs[it.x];
+        issue_tile_c2c(sg.d, static_cast<const char *>(bufs.p[sg.in_buf]) + sg.in_off, sm, it.y);
+    }
+    cp_async_commit();
+    for (int i = 0; w < nitems; i++) {
+        float2 *cur = sm + (i & 1) * span;
+        // dequeue the next item and prefetch it into the other buffer when possible
+        __syncthreads();  // everyone has read s_item / s_pref of the current item
+        if (tid == 0) {
+            s_item = atomicAdd(counter, 1);
+            s_pref = 0;
+            if (s_item < nitems) {
+                const BatchSeg &nsg = segs[items[s_item].x];
+                s_pref = nsg.d.io == IO_C2C && batch_dep_done(segs, done, nsg);
+            }
+        }
+        __syncthreads();
+        const int wn = s_item;
+        const bool pref_n = s_pref != 0;
+        if (wn < nitems && pref_n) {
+            const int2 itn = items[wn];
+            const BatchSeg &nsg = segs[itn.x];
+            issue_tile_c2c(nsg.d, static_cast<const char *>(bufs.p[nsg.in_buf]) + nsg.in_off, sm + ((i + 1) & 1) * span,
+                           itn.y);
+        }
+        cp_async_commit();
+
+        const int2 it = items[w];
+        const BatchSeg &sg = segs[it.x];
+        const char *in = static_cast<const char *>(bufs.p[sg.in_buf]) + sg.in_off;
+        char *out = static_cast<char *>(bufs.p[sg.out_buf]) + sg.out_off;
+        bool ok = true;
+        if (!pref) {
+            if (tid == 0) s_ok = batch_dep_wait(segs, done, sg, err) ? 1 : 0;
+            __syncthreads();
+            ok = s_ok != 0;
+        }
+        cp_async_wait<1>();  // the current item's copies (if prefetched) have landed
+        __syncthreads();
+        if (ok) {
+            // a Bluestein segment runs its convolution FFTs in both directions; the
+            // other direction is conj(DFT(conj(y))) around this kernel's stages
+            process_tile<MAXE, FWD>(sg.d, in, out, it.y, cur, sg.fwd != (FWD ? 1 : 0), pref);
+            if (tid == 0) {
+                __threadfence();
+                atomicAdd(done + it.x, 1);
+            }
+        }
+        w = wn;
+        pref = pref_n;
+    }
+    cp_async_wait<0>();
 }
 
 // ------------------------------------------------------------------------------------ twiddles
@@ -385,7 +462,8 @@ void tile_kernel_fns(std::vector<const void *> &out)
     out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<16, false>));
     out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<32, true>));
     out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<32, false>));
-    out.push_back(reinterpret_cast<const void *>(batch_fft_kernel<32>));
+    out.push_back(batch_kernel_fn(true));
+    out.push_back(batch_kernel_fn(false));
     for (int maxe : {8, 16, 32})
         for (int f = 0; f < 2; f++) out.push_back(tile_db_kernel_fn(maxe, f != 0));
 }
@@ -424,14 +502,19 @@ cudaError_t launch_tile(const TileDesc &d, int maxe, bool forward, int grid, cud
     return forward ? launch_one<32, true>(d, grid, block, smem, st) : launch_one<32, false>(d, grid, block, smem, st);
 }
 
-const void *batch_kernel_fn() { return reinterpret_cast<const void *>(batch_fft_kernel<32>); }
+const void *batch_kernel_fn(bool forward)
+{
+    return forward ? reinterpret_cast<const void *>(batch_fft_kernel<kBatchMaxe, true>)
+                   : reinterpret_cast<const void *>(batch_fft_kernel<kBatchMaxe, false>);
+}
 
 cudaError_t launch_batch(int grid, int block, size_t smem, const BatchSeg *segs, const int2 *items, int nitems,
-                         int *counter, int *done, const BatchBufs &bufs, int *err, cudaStream_t st)
+                         int *counter, int *done, const BatchBufs &bufs, int *err, bool forward, cudaStream_t st)
 {
-    const void *fn = batch_kernel_fn();
+    const void *fn = batch_kernel_fn(forward);
     BatchBufs b = bufs;
-    void *args[] = {&segs, &items, &nitems, &counter, &done, &b, &err};
+    int64_t span = static_cast<int64_t>(smem / 2 / sizeof(float2));  // float2 per buffer
+    void *args[] = {&segs, &items, &nitems, &counter, &done, &b, &err, &span};
     return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, smem, st);
 }
 

@@ -53,18 +53,20 @@ struct TileCfg {
 
 // Threads, transforms per CTA and shared-memory pitch for one tile launch.
 bool choose_cfg(int n, bool column, int64_t ncols, TileCfg &c, std::string &err, int maxe_override = 0,
-                int row_threads = kRowThreadsTarget, int row_smem = kRowSmemTarget)
+                int row_threads = kRowThreadsTarget, int row_smem = kRowSmemTarget, int max_maxe = 32,
+                int max_threads = 512)
 {
     if (n < 1 || n > 32768) {
         err = "transform length out of the single-CTA range";
         return false;
     }
     c.maxe = n <= 4096 ? 16 : 32;
+    if (c.maxe > max_maxe) c.maxe = max_maxe;
     if (maxe_override == 8 || maxe_override == 16 || maxe_override == 32) {
-        if ((n + maxe_override - 1) / maxe_override <= kMaxThreads) c.maxe = maxe_override;
+        if ((n + maxe_override - 1) / maxe_override <= max_threads) c.maxe = maxe_override;
     }
     c.tpt = std::max(1, (n + c.maxe - 1) / c.maxe);
-    if (c.tpt > kMaxThreads) {
+    if (c.tpt > max_threads) {
         err = "too many threads per transform";
         return false;
     }
@@ -73,7 +75,7 @@ bool choose_cfg(int n, bool column, int64_t ncols, TileCfg &c, std::string &err,
     if (column) {
         c.tb = 0;
         for (int tb = kColTile; tb >= 1; tb /= 2) {
-            if (tb * c.tpt <= kMaxThreads && tb * bytes_per <= kMaxSmemBytes) {
+            if (tb * c.tpt <= max_threads && tb * bytes_per <= kMaxSmemBytes) {
                 c.tb = tb;
                 break;
             }
@@ -82,7 +84,7 @@ bool choose_cfg(int n, bool column, int64_t ncols, TileCfg &c, std::string &err,
         int tb = std::max(1, row_threads / c.tpt);
         while (tb > 1 && tb * bytes_per > row_smem) tb /= 2;
         if (tb > ncols) tb = static_cast<int>(std::max<int64_t>(1, ncols));
-        while (tb > 1 && tb * c.tpt > kMaxThreads) tb /= 2;
+        while (tb > 1 && tb * c.tpt > max_threads) tb /= 2;
         c.tb = (bytes_per <= kMaxSmemBytes) ? tb : 0;
     }
     if (c.tb == 0) {
@@ -197,12 +199,14 @@ struct Builder {
         }
         int maxe_override = 0;
         TuneChoice tc;
-        if (p.use_tuned && tuned_choice(n, tc) && valid_radices(tc.radices, n)) {
+        if (p.use_tuned && tuned_choice(n, tc) && valid_radices(tc.radices, n) && tc.maxe <= p.max_maxe) {
             radices = tc.radices;
             maxe_override = tc.maxe;
         }
         TileCfg c;
-        if (!choose_cfg(n, column, n_cols, c, err, maxe_override, p.row_threads, p.row_smem)) return false;
+        if (!choose_cfg(n, column, n_cols, c, err, maxe_override, p.row_threads, p.row_smem, p.max_maxe,
+                        p.max_maxe < 32 ? p.row_threads : kMaxThreads))
+            return false;
         s = Step();
         s.kind = StepKind::kTile;
         s.forward = fwd;
@@ -505,7 +509,7 @@ struct Builder {
         const bool smooth = factor_radices(n, probe);
         if (inner == 1 && !smooth) return add_bluestein(0, n, outer, n, n, src, dst);
         if (inner == 1) {
-            if (n <= kMaxRowN) {
+            if (n <= std::min<int64_t>(kMaxRowN, p.max_row_n)) {
                 const float2 *tw = table(n, n);
                 if (!tw) return false;
                 Addr a{0, n, 1, 0, 0};

@@ -42,10 +42,15 @@ cudaError_t configure_kernels(int device);
 void tile_kernel_fns(std::vector<const void *> &out);
 void row_kernel_fns(std::vector<const void *> &out);
 void static_kernel_fns(std::vector<const void *> &out);
-// persistent uneven-batch kernel (fft_tile.cu)
-const void *batch_kernel_fn();
+// persistent uneven-batch kernel (fft_tile.cu): CTAs of kBatchBlock threads, at
+// most kBatchMaxe points per thread; batch plans keep single-tile rows at or
+// below kBatchMaxRowN (longer rows are multi-pass) so several CTAs fit per SM
+constexpr int kBatchBlock = 256;
+constexpr int kBatchMaxe = 16;
+constexpr int64_t kBatchMaxRowN = 4096;
+const void *batch_kernel_fn(bool forward);
 cudaError_t launch_batch(int grid, int block, size_t smem, const BatchSeg *segs, const int2 *items, int nitems,
-                         int *counter, int *done, const BatchBufs &bufs, int *err, cudaStream_t st);
+                         int *counter, int *done, const BatchBufs &bufs, int *err, bool forward, cudaStream_t st);
 cudaError_t launch_kernel_fn(const void *fn, const TileDesc &d, int grid, size_t smem, int *err, cudaStream_t st);
 
 // Compile-time specialised pipelined row kernels (static_fft.cu).
@@ -181,6 +186,8 @@ struct Plan {
     bool use_tuned = false;  // consult the autotuner's choices (uneven-batch plans)
     int row_threads = 256;   // threads per CTA the row tiles aim for
     int row_smem = 64 * 1024;  // shared memory per CTA the row tiles stay under
+    int64_t max_row_n = 1 << 30;  // C2C rows longer than this take the multi-pass path
+    int max_maxe = 32;            // largest points per thread a tile may use (tuned choices above are ignored)
     // 0: FP32 kernels; 1: tensor-core FP16 hi/lo x3; 2: tensor-core BF16 hi/lo x3
     // (lengths without a tensor-core stage keep the FP32 kernels)
     int precision = 0;
