@@ -413,7 +413,7 @@ def run_uneven(args, world, rank, local):
     from sip_b200 import fft, workloads
 
     torch.cuda.set_device(local)
-    groups = workloads.uneven_batch_set(total=20000, seed=2024)
+    groups = workloads.uneven_batch_set(total=args.uneven_total, seed=2024)
     fl, alg_bytes = workloads.uneven_flops_bytes(groups)
     cache = os.path.join(ROOT, "sip_b200", "tune", "b200_c2c_fp32.jsonl")
     if args.autotune:
@@ -445,9 +445,9 @@ def run_uneven(args, world, rank, local):
             "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "dtype": "f32",
             "data": "synthetic (seeded lengths/batches, randn values)",
-            "config": {"workload": "20000 1D C2C complex64 transforms, lengths log-uniform in [64, 65536] snapped to "
+            "config": {"workload": f"{args.uneven_total} 1D C2C complex64 transforms, lengths log-uniform in [64, 65536] snapped to "
                                    "7-smooth, Zipf(1.2) batch per length capped at 512; one persistent launch "
-                                   "replayed from a CUDA graph", "groups": len(groups), "transforms": 20000,
+                                   "replayed from a CUDA graph", "groups": len(groups), "transforms": args.uneven_total,
                        "bytes_in": alg_bytes // 2, "tuned": os.path.exists(cache)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": kind, "algorithmic_bytes_per_step": alg_bytes},
@@ -610,6 +610,7 @@ def main():
     ap.add_argument("--seconds", type=float, default=1.0)
     ap.add_argument("--max-requests", type=int, default=2000)
     ap.add_argument("--autotune", action="store_true", help="(uneven) run the autotuner and refresh its cache")
+    ap.add_argument("--uneven-total", type=int, default=20000, help="(uneven) transforms in the drawn set")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.workload == "uneven":

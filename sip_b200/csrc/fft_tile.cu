@@ -45,9 +45,9 @@ constexpr int maxv_for()
 // (tws[(r-1)*ns + j mod ns]: consecutive butterflies read consecutive
 // entries), else from the length-n table (tw[r*(j mod ns)*tstep]).
 template <int R, int MAXE, bool FWD>
-__device__ __forceinline__ void stage_read(float2 *v, const float2 *row, int n, int ns, int tstep, int lane, int tpt,
-                                           bool active, const float2 *__restrict__ tw, const float2 *__restrict__ tws,
-                                           const TileDesc &d, int64_t kc)
+__device__ __forceinline__ void stage_read(float2 *v, const float2 *row, int n, int ns, uint32_t nsm, int tstep,
+                                           int lane, int tpt, bool active, const float2 *__restrict__ tw,
+                                           const float2 *__restrict__ tws, const TileDesc &d, int64_t kc)
 {
     constexpr int NB = nb_for<R, MAXE>();
     const int nbf = n / R;
@@ -63,7 +63,7 @@ __device__ __forceinline__ void stage_read(float2 *v, const float2 *row, int n, 
                 for (int r = 0; r < R; r++) v[b * R + r] = cmul(v[b * R + r], pass_twiddle<FWD>(d, j + r * nbf, kc));
             }
             if (ns > 1) {
-                const int k = j % ns;
+                const int k = mod_ns(j, ns, nsm);
                 if (tws) {
 #pragma unroll
                     for (int r = 1; r < R; r++)
@@ -81,8 +81,8 @@ __device__ __forceinline__ void stage_read(float2 *v, const float2 *row, int n, 
 
 // Scatter the butterfly outputs to their Stockham positions.
 template <int R, int MAXE>
-__device__ __forceinline__ void stage_write(const float2 *v, float2 *row, int n, int ns, int lane, int tpt,
-                                            bool active)
+__device__ __forceinline__ void stage_write(const float2 *v, float2 *row, int n, int ns, uint32_t nsm, int lane,
+                                            int tpt, bool active)
 {
     constexpr int NB = nb_for<R, MAXE>();
     const int nbf = n / R;
@@ -90,7 +90,7 @@ __device__ __forceinline__ void stage_write(const float2 *v, float2 *row, int n,
     for (int b = 0; b < NB; b++) {
         const int j = lane + b * tpt;
         if (active && j < nbf) {
-            const int k = j % ns;
+            const int k = mod_ns(j, ns, nsm);
             const int base = (j - k) * R + k;
 #pragma unroll
             for (int r = 0; r < R; r++) row[pad(base + r * ns)] = v[b * R + r];
@@ -111,11 +111,12 @@ __device__ __forceinline__ void run_stages(float2 *row, const TileDesc &d, int l
 #pragma unroll 1
     for (int s = 0; s < d.nstages; s++) {
         const int ns = d.ns[s], ts = d.tstep[s], R = d.radix[s];
+        const uint32_t nsm = d.ns_m[s];
         const float2 *tws = d.stw ? d.stw + toff : nullptr;
         if (s > 0) toff += int64_t(R - 1) * ns;
         switch (R) {
 #define SIPFFT_READ(RR) \
-    case RR: stage_read<RR, MAXE, FWD>(v, row, d.n, ns, ts, lane, d.tpt, active, d.tw, tws, d, s == 0 ? kc : -1); break;
+    case RR: stage_read<RR, MAXE, FWD>(v, row, d.n, ns, nsm, ts, lane, d.tpt, active, d.tw, tws, d, s == 0 ? kc : -1); break;
             SIPFFT_RADIX_CASES(SIPFFT_READ)
 #undef SIPFFT_READ
             default: break;  // the planner only emits the radices above
@@ -123,7 +124,7 @@ __device__ __forceinline__ void run_stages(float2 *row, const TileDesc &d, int l
         __syncthreads();
         switch (R) {
 #define SIPFFT_WRITE(RR) \
-    case RR: stage_write<RR, MAXE>(v, row, d.n, ns, lane, d.tpt, active); break;
+    case RR: stage_write<RR, MAXE>(v, row, d.n, ns, nsm, lane, d.tpt, active); break;
             SIPFFT_RADIX_CASES(SIPFFT_WRITE)
 #undef SIPFFT_WRITE
             default: break;

@@ -42,6 +42,20 @@ struct Addr {
     int64_t cjump;
 };
 
+// j mod ns with the precomputed reciprocal m = ceil(2^32 / ns) (ns > 1), j < 2^16
+__host__ __device__ __forceinline__ int mod_ns(int j, int ns, uint32_t m)
+{
+#ifdef __CUDA_ARCH__
+    return ns == 1 ? 0 : j - static_cast<int>(__umulhi(static_cast<uint32_t>(j), m)) * ns;
+#else
+    return ns == 1 ? 0 : static_cast<int>(j - ((uint64_t(uint32_t(j)) * m) >> 32) * ns);
+#endif
+}
+__host__ __device__ constexpr uint32_t ns_reciprocal(int ns)
+{
+    return ns <= 1 ? 0u : static_cast<uint32_t>(((uint64_t(1) << 32) + uint64_t(ns) - 1) / uint64_t(ns));
+}
+
 struct TileDesc {
     const void *in;
     void *out;
@@ -51,6 +65,9 @@ struct TileDesc {
     int radix[kMaxStages];
     int ns[kMaxStages];      // product of the radices of the earlier stages
     int tstep[kMaxStages];   // twiddle table index step: (n / (ns * radix)) * tw_mul
+    // ceil(2^32 / ns) (0 when ns == 1): j mod ns = j - umulhi(j, ns_m) * ns,
+    // exact for j < 2^16 and ns < 2^16 (every butterfly index of a tile)
+    uint32_t ns_m[kMaxStages];
     int tb;         // transforms (columns) per tile
     int tpt;        // threads per transform
     int pitch;      // shared-memory floats2 per transform (padded)

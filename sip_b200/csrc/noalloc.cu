@@ -136,6 +136,7 @@ bool make_pass(TileDesc &d, int &maxe, int &grid, int rp, int64_t F, int64_t row
     for (int s = 0; s < cnt; s++) {
         d.radix[s] = radix[s];
         d.ns[s] = nsr;
+        d.ns_m[s] = ns_reciprocal(nsr);
         d.tstep[s] = rp / (nsr * radix[s]);
         nsr *= radix[s];
     }

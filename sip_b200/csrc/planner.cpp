@@ -116,6 +116,7 @@ void set_stages(TileDesc &d, const std::vector<int> &radices, int n, int tw_mul)
     for (size_t s = 0; s < radices.size(); s++) {
         d.radix[s] = radices[s];
         d.ns[s] = ns;
+        d.ns_m[s] = ns_reciprocal(ns);
         d.tstep[s] = (n / (ns * radices[s])) * tw_mul;
         ns *= radices[s];
     }

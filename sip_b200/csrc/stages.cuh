@@ -44,8 +44,8 @@ struct SmemRow {
 };
 
 template <int R, int MAXE, bool FWD, class Src>
-__device__ __forceinline__ void stage_gather(float2 *v, const Src &src, int n, int ns, int tstep, int lane, int tpt,
-                                             bool active, const float2 *__restrict__ tw,
+__device__ __forceinline__ void stage_gather(float2 *v, const Src &src, int n, int ns, uint32_t nsm, int tstep,
+                                             int lane, int tpt, bool active, const float2 *__restrict__ tw,
                                              const float2 *__restrict__ tws = nullptr)
 {
     constexpr int NB = nb_for<R, MAXE>();
@@ -64,7 +64,7 @@ __device__ __forceinline__ void stage_gather(float2 *v, const Src &src, int n, i
         if (active && j < nbf) {
             if (ns > 1) {
                 // the stage's own table when present: consecutive butterflies, consecutive entries
-                const int k = j % ns;
+                const int k = mod_ns(j, ns, nsm);
                 if (tws) {
 #pragma unroll
                     for (int r = 1; r < R; r++)
@@ -81,8 +81,8 @@ __device__ __forceinline__ void stage_gather(float2 *v, const Src &src, int n, i
 }
 
 template <int R, int MAXE, class Dst>
-__device__ __forceinline__ void stage_scatter(const float2 *v, const Dst &dst, int n, int ns, int lane, int tpt,
-                                              bool active)
+__device__ __forceinline__ void stage_scatter(const float2 *v, const Dst &dst, int n, int ns, uint32_t nsm, int lane,
+                                              int tpt, bool active)
 {
     constexpr int NB = nb_for<R, MAXE>();
     const int nbf = n / R;
@@ -90,7 +90,7 @@ __device__ __forceinline__ void stage_scatter(const float2 *v, const Dst &dst, i
     for (int b = 0; b < NB; b++) {
         const int j = lane + b * tpt;
         if (active && j < nbf) {
-            const int k = j % ns;
+            const int k = mod_ns(j, ns, nsm);
             const int base = (j - k) * R + k;
 #pragma unroll
             for (int r = 0; r < R; r++) dst(base + r * ns, v[b * R + r]);
@@ -101,12 +101,12 @@ __device__ __forceinline__ void stage_scatter(const float2 *v, const Dst &dst, i
 #define SIPFFT_RADIX_CASES(X) X(2) X(3) X(4) X(5) X(7) X(8) X(11) X(13) X(16)
 
 template <int MAXE, bool FWD, class Src>
-__device__ __forceinline__ void gather_any(int R, float2 *v, const Src &src, int n, int ns, int ts, int lane, int tpt,
-                                           bool active, const float2 *tw, const float2 *tws)
+__device__ __forceinline__ void gather_any(int R, float2 *v, const Src &src, int n, int ns, uint32_t nsm, int ts,
+                                           int lane, int tpt, bool active, const float2 *tw, const float2 *tws)
 {
     switch (R) {
 #define SIPFFT_G(RR) \
-    case RR: stage_gather<RR, MAXE, FWD>(v, src, n, ns, ts, lane, tpt, active, tw, tws); break;
+    case RR: stage_gather<RR, MAXE, FWD>(v, src, n, ns, nsm, ts, lane, tpt, active, tw, tws); break;
         SIPFFT_RADIX_CASES(SIPFFT_G)
 #undef SIPFFT_G
         default: break;
@@ -114,12 +114,12 @@ __device__ __forceinline__ void gather_any(int R, float2 *v, const Src &src, int
 }
 
 template <int MAXE, class Dst>
-__device__ __forceinline__ void scatter_any(int R, const float2 *v, const Dst &dst, int n, int ns, int lane, int tpt,
-                                            bool active)
+__device__ __forceinline__ void scatter_any(int R, const float2 *v, const Dst &dst, int n, int ns, uint32_t nsm,
+                                            int lane, int tpt, bool active)
 {
     switch (R) {
 #define SIPFFT_S(RR) \
-    case RR: stage_scatter<RR, MAXE>(v, dst, n, ns, lane, tpt, active); break;
+    case RR: stage_scatter<RR, MAXE>(v, dst, n, ns, nsm, lane, tpt, active); break;
         SIPFFT_RADIX_CASES(SIPFFT_S)
 #undef SIPFFT_S
         default: break;
@@ -147,26 +147,26 @@ __device__ __forceinline__ void run_fft(const TileDesc &d, float2 *work, const S
     // stage 0 (no twiddles); stage s >= 1 reads d.stw + toff when the plan has stage tables
     int64_t toff = 0;
     auto tws = [&](int s) -> const float2 * { return d.stw ? d.stw + toff : nullptr; };
-    gather_any<MAXE, FWD>(d.radix[0], v, src0, n, d.ns[0], d.tstep[0], lane, d.tpt, active, d.tw, nullptr);
+    gather_any<MAXE, FWD>(d.radix[0], v, src0, n, d.ns[0], d.ns_m[0], d.tstep[0], lane, d.tpt, active, d.tw, nullptr);
     if (src0_in_place || (S == 1 && dstL_in_place)) __syncthreads();
     if (S == 1) {
-        scatter_any<MAXE>(d.radix[0], v, dstL, n, d.ns[0], lane, d.tpt, active);
+        scatter_any<MAXE>(d.radix[0], v, dstL, n, d.ns[0], d.ns_m[0], lane, d.tpt, active);
         return;
     }
-    scatter_any<MAXE>(d.radix[0], v, w, n, d.ns[0], lane, d.tpt, active);
+    scatter_any<MAXE>(d.radix[0], v, w, n, d.ns[0], d.ns_m[0], lane, d.tpt, active);
     __syncthreads();
 #pragma unroll 1
     for (int s = 1; s < S - 1; s++) {
-        gather_any<MAXE, FWD>(d.radix[s], v, w, n, d.ns[s], d.tstep[s], lane, d.tpt, active, d.tw, tws(s));
+        gather_any<MAXE, FWD>(d.radix[s], v, w, n, d.ns[s], d.ns_m[s], d.tstep[s], lane, d.tpt, active, d.tw, tws(s));
         toff += int64_t(d.radix[s] - 1) * d.ns[s];
         __syncthreads();
-        scatter_any<MAXE>(d.radix[s], v, w, n, d.ns[s], lane, d.tpt, active);
+        scatter_any<MAXE>(d.radix[s], v, w, n, d.ns[s], d.ns_m[s], lane, d.tpt, active);
         __syncthreads();
     }
-    gather_any<MAXE, FWD>(d.radix[S - 1], v, w, n, d.ns[S - 1], d.tstep[S - 1], lane, d.tpt, active, d.tw,
+    gather_any<MAXE, FWD>(d.radix[S - 1], v, w, n, d.ns[S - 1], d.ns_m[S - 1], d.tstep[S - 1], lane, d.tpt, active, d.tw,
                           tws(S - 1));
     if (dstL_in_place) __syncthreads();
-    scatter_any<MAXE>(d.radix[S - 1], v, dstL, n, d.ns[S - 1], lane, d.tpt, active);
+    scatter_any<MAXE>(d.radix[S - 1], v, dstL, n, d.ns[S - 1], d.ns_m[S - 1], lane, d.tpt, active);
 }
 
 }  // namespace sipfft

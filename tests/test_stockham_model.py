@@ -36,3 +36,18 @@ def test_packed_real(n, fwd):
     assert oracle.rel_l2(sm.r2c_packed(x, fwd), oracle.r2c(x, fwd)) < 1e-12
     xh = rng.standard_normal(n // 2 + 1) + 1j * rng.standard_normal(n // 2 + 1)
     assert oracle.rel_l2(sm.c2r_packed(xh, n, fwd), oracle.c2r(xh, n, fwd)) < 1e-12
+
+
+def test_reciprocal_modulo_exact():
+    """fft_tile.cuh mod_ns: j mod ns = j - umulhi(j, ceil(2^32 / ns)) * ns for every stage
+    product ns of 7-smooth lengths up to 32768 and every butterfly index j < 2^15."""
+    import itertools
+
+    ns_values = sorted({2 ** a * 3 ** b * 5 ** c * 7 ** d
+                        for a, b, c, d in itertools.product(range(16), range(10), range(7), range(6))
+                        if 1 < 2 ** a * 3 ** b * 5 ** c * 7 ** d <= 32768})
+    j = np.arange(1 << 15, dtype=np.uint64)
+    for ns in ns_values:
+        m = np.uint64(((1 << 32) + ns - 1) // ns)
+        q = (j * m) >> np.uint64(32)
+        assert np.array_equal(j - q * np.uint64(ns), j % np.uint64(ns)), ns
