@@ -203,3 +203,29 @@ def ref_c2c_staged(x: np.ndarray, forward: bool) -> np.ndarray:
     out = np.empty_like(x)
     lib.sipref_c2c_staged(int(forward), n, x.size // n, _ptr(x), _ptr(out))
     return out
+
+
+def istft(x: np.ndarray, n_fft: int, hop: int, window: np.ndarray) -> np.ndarray:
+    """Inverse STFT as the reference computes it (center=True, normalized=False,
+    onesided=False, return_complex=True, length=None: the only values its
+    checks let through, core/fft/istft.cpp:300-390).
+
+    x: complex [channel, n_fft, n_frames] (frequency-major, as the input tensor);
+    window: real [n_fft].  Steps (core/fft/fftcore/fft_core_istft_any.cpp:292-378):
+    frames = IFFT_nfft(x[c, :, f]) / n_fft; y = overlap-add(frames * window, hop);
+    envelope = overlap-add(window^2, hop); out = (y / envelope)[n_fft/2 : L - n_fft/2]
+    with L = n_fft + hop * (n_frames - 1).
+    """
+    x = np.asarray(x, np.complex128)
+    channel, nf, n_frames = x.shape
+    assert nf == n_fft
+    w = np.asarray(window, np.float64)
+    frames = np.fft.ifft(x, axis=1)  # numpy ifft divides by n_fft: the BY_N normalisation
+    L = n_fft + hop * (n_frames - 1)
+    y = np.zeros((channel, L), np.complex128)
+    env = np.zeros(L)
+    for f in range(n_frames):
+        y[:, f * hop:f * hop + n_fft] += frames[:, :, f] * w
+        env[f * hop:f * hop + n_fft] += w * w
+    start, end = n_fft // 2, L - n_fft // 2
+    return (y / env)[:, start:end]

@@ -80,7 +80,10 @@ constexpr int64_t kMaxFftSize = int64_t(1) << 27;  // fft_api.cpp:61
 
 using namespace AsdSip;
 
-bool valid_type(int t) { return t == ASCEND_FFT_C2C || t == ASCEND_FFT_C2R || t == ASCEND_FFT_R2C; }
+bool valid_type(int t)
+{
+    return t == ASCEND_FFT_C2C || t == ASCEND_FFT_C2R || t == ASCEND_FFT_R2C || t == ASCEND_FFT_C2C_SEP;
+}
 bool valid_dir(int d) { return d == ASCEND_FFT_FORWARD || d == ASCEND_FFT_INVERSE; }
 
 int64_t prod(const std::vector<int64_t> &v)
@@ -95,7 +98,8 @@ AspbStatus finish_plan(sipfft::Plan &p, std::string (*builder)(sipfft::Plan &), 
 {
     p.steps.clear();
     p.tables.clear();
-    p.ws_buf_bytes[0] = p.ws_buf_bytes[1] = 0;
+    p.ws_buf_bytes[0] = p.ws_buf_bytes[1] = p.ws_buf_bytes[2] = 0;
+    if (builder != sipfft::build_plan_istft) p.istft = false;
     p.ws_bytes = 0;
     p.initialized = false;
     p.failed = false;
@@ -158,7 +162,8 @@ void *tensor_addr(const aclTensor *t)
     return static_cast<char *>(t->data) + t->offset * static_cast<int64_t>(dtype_size(t->dtype));
 }
 
-AspbStatus run(sipfft::Plan &p, const void *in, void *out, const char *where)
+AspbStatus run(sipfft::Plan &p, const void *in, void *out, const char *where, const float *in_im = nullptr,
+               float *out_im = nullptr)
 {
     std::lock_guard<std::mutex> lock(p.mu);
     if (!p.initialized) {
@@ -173,11 +178,21 @@ AspbStatus run(sipfft::Plan &p, const void *in, void *out, const char *where)
         log_error(where, "tensor data is null");
         return ACL_ERROR_INTERNAL_ERROR;
     }
-    if (p.fft_type != ASCEND_FFT_C2C && in == out) {
+    if (p.fft_type != ASCEND_FFT_C2C && p.fft_type != ASCEND_FFT_C2C_SEP && in == out) {
         log_error(where, "in-place execution is supported for C2C plans only");
         return ACL_ERROR_INVALID_PARAM;
     }
-    const uintptr_t align_mask = 7;
+    if (p.fft_type == ASCEND_FFT_C2C_SEP) {
+        if (!in_im || !out_im || (in == out) != (static_cast<const void *>(in_im) == out_im)) {
+            log_error(where, "separated plans need both planes, in place for both or for neither");
+            return ACL_ERROR_INVALID_PARAM;
+        }
+        if ((reinterpret_cast<uintptr_t>(in_im) & 3) || (reinterpret_cast<uintptr_t>(out_im) & 3)) {
+            log_error(where, "imaginary planes must be 4-byte aligned");
+            return ACL_ERROR_INVALID_PARAM;
+        }
+    }
+    const uintptr_t align_mask = p.fft_type == ASCEND_FFT_C2C_SEP ? 3 : 7;
     if ((reinterpret_cast<uintptr_t>(in) & align_mask) || (reinterpret_cast<uintptr_t>(out) & align_mask)) {
         log_error(where, "device buffers must be 8-byte aligned");
         return ACL_ERROR_INVALID_PARAM;
@@ -185,7 +200,7 @@ AspbStatus run(sipfft::Plan &p, const void *in, void *out, const char *where)
     int cur = 0;
     cudaGetDevice(&cur);
     if (cur != p.device) cudaSetDevice(p.device);
-    cudaError_t e = sipfft::execute_plan(p, in, out, static_cast<cudaStream_t>(p.stream));
+    cudaError_t e = sipfft::execute_plan(p, in, out, static_cast<cudaStream_t>(p.stream), in_im, out_im);
     if (cur != p.device) cudaSetDevice(cur);
     if (e != cudaSuccess) {
         log_error(where, cudaGetErrorString(e));
@@ -290,8 +305,7 @@ AspbStatus asdFftMakePlan1D(asdFftHandle handle, int64_t fftSize, enum asdFftTyp
     sipfft::Plan *p = find_plan(handle);
     if (!p) return ACL_ERROR_INVALID_PARAM;
     if (fftSize <= 0 || fftSize > kMaxFftSize || batchSize <= 0) return ACL_ERROR_INVALID_PARAM;
-    if (fftType == ASCEND_FFT_C2C_SEP || fftType == ASCEND_STFT_C2C || fftType == ASCEND_STFT_C2R ||
-        fftType == ASCEND_STFT_R2C)
+    if (fftType == ASCEND_STFT_C2C || fftType == ASCEND_STFT_C2R || fftType == ASCEND_STFT_R2C)
         return ACL_ERROR_API_NOT_SUPPORT;
     if (!valid_type(fftType) || !valid_dir(direction)) return ACL_ERROR_INVALID_PARAM;
     const bool vertical = dimType == ASCEND_FFT_VERTICAL;
@@ -315,8 +329,7 @@ AspbStatus asdFftMakePlan2D(asdFftHandle handle, int64_t fftSizeX, int64_t fftSi
     if (!p) return ACL_ERROR_INVALID_PARAM;
     if (fftSizeX <= 0 || fftSizeX > kMaxFftSize || fftSizeY <= 0 || fftSizeY > kMaxFftSize || batchSize <= 0)
         return ACL_ERROR_INVALID_PARAM;
-    if (fftType == ASCEND_FFT_C2C_SEP || fftType == ASCEND_STFT_C2C || fftType == ASCEND_STFT_C2R ||
-        fftType == ASCEND_STFT_R2C)
+    if (fftType == ASCEND_STFT_C2C || fftType == ASCEND_STFT_C2R || fftType == ASCEND_STFT_R2C)
         return ACL_ERROR_API_NOT_SUPPORT;
     if (!valid_type(fftType) || !valid_dir(direction)) return ACL_ERROR_INVALID_PARAM;
     std::lock_guard<std::mutex> lock(p->mu);
@@ -337,8 +350,7 @@ AspbStatus asdFftMakePlan3D(asdFftHandle handle, int64_t fftSizeX, int64_t fftSi
     if (fftSizeX <= 0 || fftSizeX > kMaxFftSize || fftSizeY <= 0 || fftSizeY > kMaxFftSize || fftSizeZ <= 0 ||
         fftSizeZ > kMaxFftSize || batchSize <= 0)
         return ACL_ERROR_INVALID_PARAM;
-    if (fftType == ASCEND_FFT_C2C_SEP || fftType == ASCEND_STFT_C2C || fftType == ASCEND_STFT_C2R ||
-        fftType == ASCEND_STFT_R2C)
+    if (fftType == ASCEND_STFT_C2C || fftType == ASCEND_STFT_C2R || fftType == ASCEND_STFT_R2C)
         return ACL_ERROR_API_NOT_SUPPORT;
     if (!valid_type(fftType) || !valid_dir(direction)) return ACL_ERROR_INVALID_PARAM;
     std::lock_guard<std::mutex> lock(p->mu);
@@ -351,30 +363,147 @@ AspbStatus asdFftMakePlan3D(asdFftHandle handle, int64_t fftSizeX, int64_t fftSi
     return finish_plan(*p, sipfft::build_plan_3d, "asdFftMakePlan3D");
 }
 
-AspbStatus asdFftIstftMakePlan(asdFftHandle handle, const aclTensor *, const int64_t, const int64_t, const int64_t,
-                               const bool, const bool, const bool, int64_t, const bool)
+// core/fft/istft.cpp:300-390 (IstftParamsCheck) and 530-552: options the
+// reference does not support are forced to center = true, normalized = false,
+// onesided = false, length = 0, return_complex = true with a warning; the
+// input is complex64 [channel, n_fft, frames] with frames > 1; 0 < hop <= win
+// length == n_fft; n_fft and hop below 1500.  The plan is an INVERSE C2C plan
+// (GetType reports C2C) whose workspace holds the transformed frames.
+AspbStatus asdFftIstftMakePlan(asdFftHandle handle, const aclTensor *input, const int64_t nFft,
+                               const int64_t hopLengthOpt, const int64_t winLengthOpt, const bool center,
+                               const bool normalized, const bool onesidedOpt, int64_t lengthOpt, const bool returnComplex)
 {
-    if (!find_plan(handle)) return ACL_ERROR_INVALID_PARAM;
-    return ACL_ERROR_API_NOT_SUPPORT;
+    constexpr int64_t kMaxIstft = 1500;  // istft.cpp:32-33
+    sipfft::Plan *p = find_plan(handle);
+    if (!p) return ACL_ERROR_INVALID_PARAM;
+    const char *where = "asdFftIstftMakePlan";
+    if (!input || input->dtype != ACL_COMPLEX64 || input->view.size() != 3) {
+        log_error(where, "input must be a 3-dimensional complex64 tensor [channel, n_fft, frames]");
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    if (!center) log_error(where, "warning: only center = true is supported; using it");
+    if (normalized) log_error(where, "warning: only normalized = false is supported; using it");
+    if (onesidedOpt) log_error(where, "warning: only onesided = false is supported; using it");
+    if (!returnComplex) log_error(where, "warning: only return_complex = true is supported; using it");
+    if (lengthOpt != 0) log_error(where, "warning: only length = 0 is supported; using it");
+    const int64_t channel = input->view[0], fft_size = input->view[1], frames = input->view[2];
+    if (channel <= 0 || frames <= 1 || nFft != fft_size || !(0 < hopLengthOpt && hopLengthOpt <= winLengthOpt) ||
+        !(winLengthOpt > 0 && winLengthOpt == nFft) || nFft >= kMaxIstft || hopLengthOpt >= kMaxIstft) {
+        log_error(where, "parameters outside the supported ISTFT range");
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    std::lock_guard<std::mutex> lock(p->mu);
+    p->fft_type = ASCEND_FFT_C2C;
+    p->direction = ASCEND_FFT_INVERSE;
+    p->sizes = {nFft};
+    p->strides = {frames};
+    p->vertical = false;
+    p->batch = channel * frames;
+    p->istft = true;
+    p->istft_channel = channel;
+    p->istft_frames = frames;
+    p->istft_nfft = nFft;
+    p->istft_hop = hopLengthOpt;
+    p->istft_out_len = nFft + hopLengthOpt * (frames - 1) - 2 * (nFft / 2);  // istft.cpp:245-260
+    return finish_plan(*p, sipfft::build_plan_istft, where);
 }
 
-AspbStatus asdFftExecIstft(asdFftHandle handle, const aclTensor *, const aclTensor *, const aclTensor *)
+// core/fft/istft.cpp:554-575 and the checks it calls: input as recorded at
+// plan time, window float32 [n_fft], output complex64 [channel, out_len].
+AspbStatus asdFftExecIstft(asdFftHandle handle, const aclTensor *input, const aclTensor *windowOpt,
+                           const aclTensor *output)
 {
-    if (!find_plan(handle)) return ACL_ERROR_INVALID_PARAM;
-    return ACL_ERROR_API_NOT_SUPPORT;
+    sipfft::Plan *p = find_plan(handle);
+    if (!p) return ACL_ERROR_INVALID_PARAM;
+    const char *where = "asdFftExecIstft";
+    std::lock_guard<std::mutex> lock(p->mu);
+    if (!p->istft || !p->initialized) {
+        log_error(where, "the handle holds no initialised ISTFT plan");
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    if (!input || input->dtype != ACL_COMPLEX64 || input->view.size() != 3 || input->view[0] != p->istft_channel ||
+        input->view[1] != p->istft_nfft || input->view[2] != p->istft_frames) {
+        log_error(where, "input does not match the ISTFT plan");
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    if (!output || output->dtype != ACL_COMPLEX64 || output->view.size() != 2 ||
+        output->view[0] != p->istft_channel || output->view[1] != p->istft_out_len) {
+        log_error(where, "output must be complex64 [channel, n_fft + hop (frames - 1) - 2 (n_fft / 2)]");
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    if (!windowOpt || windowOpt->dtype != ACL_FLOAT || windowOpt->view.size() != 1 ||
+        windowOpt->view[0] != p->istft_nfft) {
+        log_error(where, "window must be float32 [n_fft]");
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    if (p->ws_bytes > 0 && p->workspace == nullptr) {
+        log_error(where, "workspace has not been set");
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    const void *in = input->data ? tensor_addr(input) : nullptr;
+    const void *win = windowOpt->data ? tensor_addr(windowOpt) : nullptr;
+    void *out = output->data ? tensor_addr(output) : nullptr;
+    if (!in || !win || !out) {
+        log_error(where, "tensor data is null");
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    if ((reinterpret_cast<uintptr_t>(in) & 7) || (reinterpret_cast<uintptr_t>(out) & 7) ||
+        (reinterpret_cast<uintptr_t>(win) & 3)) {
+        log_error(where, "misaligned device buffer");
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p->device) cudaSetDevice(p->device);
+    cudaStream_t st = static_cast<cudaStream_t>(p->stream);
+    cudaError_t e = sipfft::execute_plan(*p, in, out, st);
+    if (e == cudaSuccess)
+        e = sipfft::launch_istft_ola(static_cast<const float2 *>(p->workspace), static_cast<const float *>(win),
+                                     static_cast<float2 *>(out), p->istft_channel, static_cast<int>(p->istft_frames),
+                                     static_cast<int>(p->istft_nfft), static_cast<int>(p->istft_hop),
+                                     p->istft_out_len, st);
+    if (cur != p->device) cudaSetDevice(cur);
+    if (e != cudaSuccess) {
+        log_error(where, cudaGetErrorString(e));
+        cudaGetLastError();
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    return ACL_SUCCESS;
 }
 
-AspbStatus asdFftExecC2CSeparated(asdFftHandle handle, const aclTensor *, const aclTensor *, const aclTensor *,
-                                  const aclTensor *)
+// fft_api.cpp:1281-1342: the four planes must have the same rank and shape
+// (else 500000); the plan must be an ASCEND_FFT_C2C_SEP plan.
+AspbStatus asdFftExecC2CSeparated(asdFftHandle handle, const aclTensor *inputReal, const aclTensor *inputImag,
+                                  const aclTensor *outputReal, const aclTensor *outputImag)
 {
-    if (!find_plan(handle)) return ACL_ERROR_INVALID_PARAM;
-    return ACL_ERROR_API_NOT_SUPPORT;
+    sipfft::Plan *p = find_plan(handle);
+    if (!p) return ACL_ERROR_INVALID_PARAM;
+    const aclTensor *t[4] = {inputReal, inputImag, outputReal, outputImag};
+    for (const aclTensor *x : t)
+        if (!x || !x->data) {
+            log_error("asdFftExecC2CSeparated", "tensor data is null");
+            return ACL_ERROR_INTERNAL_ERROR;
+        }
+    for (int i = 1; i < 4; i++)
+        if (t[i]->view != t[0]->view) {
+            log_error("asdFftExecC2CSeparated", "input/output planes differ in shape");
+            return ACL_ERROR_INTERNAL_ERROR;
+        }
+    if (p->initialized && p->fft_type != ASCEND_FFT_C2C_SEP) return ACL_ERROR_INVALID_PARAM;
+    for (const aclTensor *x : t)
+        if (!match_tensor(*p, x, 2)) {
+            log_error("asdFftExecC2CSeparated", "planes do not match plan (float32, trailing dims = sizes)");
+            return ACL_ERROR_INVALID_PARAM;
+        }
+    return run(*p, tensor_addr(inputReal), tensor_addr(outputReal), "asdFftExecC2CSeparated",
+               static_cast<const float *>(tensor_addr(inputImag)), static_cast<float *>(tensor_addr(outputImag)));
 }
 
 AspbStatus asdFftExecC2C(asdFftHandle handle, const aclTensor *input, const aclTensor *output)
 {
     sipfft::Plan *p = find_plan(handle);
     if (!p) return ACL_ERROR_INVALID_PARAM;
+    if (p->istft) return ACL_ERROR_INVALID_PARAM;  // an ISTFT plan runs through asdFftExecIstft
     if (p->initialized && p->fft_type != ASCEND_FFT_C2C) return ACL_ERROR_INVALID_PARAM;
     if (!match_tensor(*p, input, 0) || !match_tensor(*p, output, 0)) {
         log_error("asdFftExecC2C", "input/output does not match plan");
@@ -387,6 +516,7 @@ AspbStatus asdFftExecC2R(asdFftHandle handle, const aclTensor *input, const aclT
 {
     sipfft::Plan *p = find_plan(handle);
     if (!p) return ACL_ERROR_INVALID_PARAM;
+    if (p->istft) return ACL_ERROR_INVALID_PARAM;  // an ISTFT plan runs through asdFftExecIstft
     if (p->initialized && p->fft_type != ASCEND_FFT_C2R) return ACL_ERROR_INVALID_PARAM;
     if (!match_tensor(*p, input, 1) || !match_tensor(*p, output, 2)) {
         log_error("asdFftExecC2R", "input/output does not match plan");
@@ -399,6 +529,7 @@ AspbStatus asdFftExecR2C(asdFftHandle handle, const aclTensor *input, const aclT
 {
     sipfft::Plan *p = find_plan(handle);
     if (!p) return ACL_ERROR_INVALID_PARAM;
+    if (p->istft) return ACL_ERROR_INVALID_PARAM;  // an ISTFT plan runs through asdFftExecIstft
     if (p->initialized && p->fft_type != ASCEND_FFT_R2C) return ACL_ERROR_INVALID_PARAM;
     if (!match_tensor(*p, input, 2) || !match_tensor(*p, output, 1)) {
         log_error("asdFftExecR2C", "input/output does not match plan");

@@ -100,6 +100,12 @@ struct TileDesc {
     const float2 *bmul;
     int blue_n;
     int blue_kind;
+    // Planar (separated) complex data: bit 0 = input, bit 1 = output.  The
+    // real plane is in / out (float), the imaginary plane in_im / out_im,
+    // both indexed like the interleaved layout's complex elements.
+    int planar;
+    const float *in_im;
+    float *out_im;
 };
 
 // One segment of an uneven batch: a tile-kernel step whose source and

@@ -176,8 +176,52 @@ struct Builder {
 
     void need_ws(Buf b, size_t bytes)
     {
-        const int i = b == Buf::kWs0 ? 0 : 1;
+        const int i = b == Buf::kWs0 ? 0 : (b == Buf::kWs1 ? 1 : 2);
         p.ws_buf_bytes[i] = std::max(p.ws_buf_bytes[i], bytes);
+    }
+
+    // ASCEND_FFT_C2C_SEP: the C2C steps with separated real / imaginary user
+    // planes.  The first step reads the planes, the last writes them; any
+    // intermediate that the interleaved plan keeps in the user output (which
+    // holds only the real plane here) moves to workspace slot 2.
+    bool make_planar()
+    {
+        const size_t S = p.steps.size();
+        if (S == 0) return false;
+        int64_t elems = p.batch;
+        for (int64_t v : p.sizes) elems *= v;
+        bool redirect = false;
+        for (size_t i = 0; i < S; i++) {
+            Step &s = p.steps[i];
+            const bool ok_io = s.d.io == IO_C2C || (i == 0 && s.d.io == IO_BLUE_PRE && s.d.blue_kind == 0) ||
+                               (i + 1 == S && s.d.io == IO_BLUE_POST && s.d.blue_kind == 0);
+            if (s.kind != StepKind::kTile || !ok_io) {
+                err = "separated layout supports C2C steps only";
+                return false;
+            }
+            if (i + 1 < S && s.dst == Buf::kUserOut) {
+                s.dst = Buf::kWs2;
+                redirect = true;
+            }
+            if (i > 0 && s.src == Buf::kUserOut) s.src = Buf::kWs2;
+            if (i > 0 && s.src == Buf::kUserIn) {
+                err = "separated layout: a later step reads the user input";
+                return false;
+            }
+        }
+        p.steps.front().d.planar |= 1;
+        if (p.steps.back().dst == Buf::kUserOut) p.steps.back().d.planar |= 2;
+        for (Step &s : p.steps) {
+            if (!s.d.planar) continue;
+            // the planar load / store phases live in the tile kernel only
+            s.has_row = false;
+            s.row_fn = nullptr;
+            s.db = false;
+            s.tc_fmt = -1;
+            s.what += " [separated re/im]";
+        }
+        if (redirect) need_ws(Buf::kWs2, size_t(elems) * sizeof(float2));
+        return true;
     }
 
     // One single-CTA launch over a set of transforms.
@@ -251,7 +295,7 @@ struct Builder {
                 s.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(d.num_tiles, int64_t(per_sm) * sm_count(device))));
             }
         }
-        if (p.precision != 0 && (io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
+        if (p.precision != 0 && p.fft_type != 0x30 && (io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
             return add_tc_variant(s);
         return true;
     }
@@ -637,10 +681,14 @@ std::string finish(Plan &p, Builder &b, bool ok)
         p.steps.clear();
         return b.err.empty() ? std::string("planning failed") : b.err;
     }
+    if (p.fft_type == 0x30 && !b.make_planar()) {
+        p.steps.clear();
+        return b.err;
+    }
     p.ws_bytes = 0;
-    if (p.ws_buf_bytes[0] || p.ws_buf_bytes[1]) {
+    if (p.ws_buf_bytes[0] || p.ws_buf_bytes[1] || p.ws_buf_bytes[2]) {
         auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-        p.ws_bytes = al(p.ws_buf_bytes[0]) + al(p.ws_buf_bytes[1]);
+        p.ws_bytes = al(p.ws_buf_bytes[0]) + al(p.ws_buf_bytes[1]) + al(p.ws_buf_bytes[2]);
     }
     return std::string();
 }
@@ -689,6 +737,7 @@ std::string build_plan_1d(Plan &p)
     const int64_t n = p.sizes[0];
     bool ok = false;
     switch (p.fft_type) {
+        case 0x30:  // C2C on separated planes (converted after planning)
         case 0x10:  // C2C
             ok = p.vertical ? b.axis_c2c(n, 1, p.batch, Buf::kUserIn, Buf::kUserOut)
                             : b.axis_c2c(n, p.batch, 1, Buf::kUserIn, Buf::kUserOut);
@@ -712,6 +761,7 @@ std::string build_plan_2d(Plan &p)
     const int64_t Yh = Y / 2 + 1;
     bool ok = false;
     switch (p.fft_type) {
+        case 0x30:
         case 0x10:
             ok = b.axis_c2c(Y, B * X, 1, Buf::kUserIn, Buf::kUserOut) &&
                  b.axis_c2c(X, B, Y, Buf::kUserOut, Buf::kUserOut);
@@ -737,6 +787,7 @@ std::string build_plan_3d(Plan &p)
     const int64_t Zh = Z / 2 + 1;
     bool ok = false;
     switch (p.fft_type) {
+        case 0x30:
         case 0x10:
             ok = b.axis_c2c(Z, B * X * Y, 1, Buf::kUserIn, Buf::kUserOut) &&
                  b.axis_c2c(Y, B * X, Z, Buf::kUserOut, Buf::kUserOut) &&
@@ -756,6 +807,28 @@ std::string build_plan_3d(Plan &p)
         default:
             b.err = "unsupported transform type";
     }
+    return finish(p, b, ok);
+}
+
+// Inverse STFT (core/fft/istft.cpp:495-575): the reference transposes
+// [channel, n_fft, frames] to [channel, frames, n_fft] and runs an INVERSE C2C
+// plan over the frames; here one column-tile step reads the frequency-major
+// input in place and writes the frames in [channel][frame][n_fft] order into
+// workspace slot 0, where the overlap-add kernel reads them.
+std::string build_plan_istft(Plan &p)
+{
+    Builder b(p);
+    const int64_t n = p.istft_nfft, F = p.istft_frames, C = p.istft_channel;
+    std::vector<int> probe;
+    if (!factor_radices(n, probe)) return "ISTFT length " + std::to_string(n) + " has a prime factor above 13";
+    const float2 *tw = b.table(n, n);
+    if (!tw) return b.err;
+    std::ostringstream w;
+    w << "ISTFT frames: inverse C2C n=" << n << " channels=" << C << " frames=" << F;
+    b.need_ws(Buf::kWs0, size_t(C) * F * n * sizeof(float2));
+    const Addr ia{n * F, 1, F, 0, 0};  // element e of frame f of channel c at c n F + f + e F
+    const Addr oa{F * n, n, 1, 0, 0};  // written at c F n + f n + e
+    const bool ok = b.add_tile(IO_C2C, static_cast<int>(n), 1, tw, true, C, F, ia, oa, Buf::kUserIn, Buf::kWs0, w.str());
     return finish(p, b, ok);
 }
 

@@ -217,20 +217,18 @@ bool scale_steps_to_rows(const Plan &p, int64_t rows, std::vector<Step> &out)
     return true;
 }
 
-cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const void *in, void *out, void *workspace,
-                          cudaStream_t st);
-
-cudaError_t execute_plan(Plan &p, const void *in, void *out, cudaStream_t st)
+cudaError_t execute_plan(Plan &p, const void *in, void *out, cudaStream_t st, const float *in_im, float *out_im)
 {
-    return execute_steps(p, p.steps, in, out, p.workspace, st);
+    return execute_steps(p, p.steps, in, out, p.workspace, st, in_im, out_im);
 }
 
 cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const void *in, void *out, void *workspace,
-                          cudaStream_t st)
+                          cudaStream_t st, const float *in_im, float *out_im)
 {
     char *ws = static_cast<char *>(workspace);
     const size_t off1 = (p.ws_buf_bytes[0] + 255) / 256 * 256;
-    void *bufs[4] = {const_cast<void *>(in), out, ws, ws ? ws + off1 : nullptr};
+    const size_t off2 = off1 + (p.ws_buf_bytes[1] + 255) / 256 * 256;
+    void *bufs[5] = {const_cast<void *>(in), out, ws, ws ? ws + off1 : nullptr, ws ? ws + off2 : nullptr};
     for (const Step &s : steps) {
         const void *src = bufs[static_cast<int>(s.src)];
         void *dst = bufs[static_cast<int>(s.dst)];
@@ -266,6 +264,9 @@ cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const v
                     TileDesc d = s.d;
                     d.in = src;
                     d.out = dst;
+                    d.in_im = in_im;
+                    d.out_im = out_im;
+                    if ((d.planar & 1 && !in_im) || (d.planar & 2 && !out_im)) return cudaErrorInvalidDevicePointer;
                     e = launch_tile(d, s.maxe, s.forward, s.grid, st);
                 }
                 break;

@@ -89,6 +89,9 @@ cudaError_t fill_tc_bmatrix(uint16_t *hi, uint16_t *lo, int N, int fmt, bool fwd
 cudaError_t launch_tc_rows(int n, int fmt, bool fwd, const float2 *in, float2 *out, int64_t rows, int64_t in_dist,
                            int64_t out_dist, const uint16_t *fa, const uint16_t *fb, const float2 *tw, int grid,
                            int *err, cudaStream_t st);
+// Overlap-add, window envelope and centre slice of the inverse STFT (istft.cu).
+cudaError_t launch_istft_ola(const float2 *frames, const float *window, float2 *out, int64_t channel, int n_frames,
+                             int n_fft, int hop, int64_t out_len, cudaStream_t st);
 // Process-wide device error word of the current device (bounded waits that
 // gave up set it); read and cleared by asdFftSynchronize.
 int *device_error_word(int device);
@@ -125,7 +128,7 @@ TablePtr get_stage_table(const int *radix, int nstages, int device, std::string 
 // ptr, lo at ptr + N^2 float2, each 2N x 2N 16-bit values.
 TablePtr get_tc_matrix(int N, int fmt, bool fwd, int device, std::string *err, int layout = 0);
 
-enum class Buf : int { kUserIn = 0, kUserOut = 1, kWs0 = 2, kWs1 = 3 };
+enum class Buf : int { kUserIn = 0, kUserOut = 1, kWs0 = 2, kWs1 = 3, kWs2 = 4 };
 
 enum class StepKind : int { kTile = 0, kR2CPost = 1, kC2RPre = 2 };
 
@@ -179,7 +182,7 @@ struct Plan {
     // build-specific
     int device = 0;
     std::vector<Step> steps;
-    size_t ws_buf_bytes[2] = {0, 0};
+    size_t ws_buf_bytes[3] = {0, 0, 0};
     size_t ws_bytes = 0;
     std::vector<TablePtr> tables;
     std::mutex mu;
@@ -188,6 +191,10 @@ struct Plan {
     int row_smem = 64 * 1024;  // shared memory per CTA the row tiles stay under
     int64_t max_row_n = 1 << 30;  // C2C rows longer than this take the multi-pass path
     int max_maxe = 32;            // largest points per thread a tile may use (tuned choices above are ignored)
+    // inverse STFT plan (asdFftIstftMakePlan): one column C2C step into workspace
+    // slot 0 ([channel][frame][n_fft]), then the overlap-add kernel
+    bool istft = false;
+    int64_t istft_channel = 0, istft_frames = 0, istft_nfft = 0, istft_hop = 0, istft_out_len = 0;
     // 0: FP32 kernels; 1: tensor-core FP16 hi/lo x3; 2: tensor-core BF16 hi/lo x3
     // (lengths without a tensor-core stage keep the FP32 kernels)
     int precision = 0;
@@ -205,11 +212,14 @@ bool save_tune_cache(const std::string &path, int device);
 std::string build_plan_1d(Plan &p);
 std::string build_plan_2d(Plan &p);
 std::string build_plan_3d(Plan &p);
+std::string build_plan_istft(Plan &p);
 // Launch every step of an initialised plan.
-cudaError_t execute_plan(Plan &p, const void *in, void *out, cudaStream_t st);
+cudaError_t execute_plan(Plan &p, const void *in, void *out, cudaStream_t st, const float *in_im = nullptr,
+                         float *out_im = nullptr);
 // Same for an explicit step list (e.g. re-targeted to fewer rows) and workspace.
+// in_im / out_im: imaginary planes of a planar (ASCEND_FFT_C2C_SEP) plan's user buffers.
 cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const void *in, void *out, void *workspace,
-                          cudaStream_t st);
+                          cudaStream_t st, const float *in_im = nullptr, float *out_im = nullptr);
 bool scale_steps_to_rows(const Plan &p, int64_t rows, std::vector<Step> &out);
 std::string describe_plan(const Plan &p);
 

@@ -176,7 +176,8 @@ struct FusedR2C {
 template <class Q, int T>
 struct StaticEngine {
     static constexpr int kMaxThreads = T <= 256 ? 256 : T;
-    static constexpr int kMinBlocks = T <= 256 ? 3 : 1;
+    // 3 CTAs per SM (<= 80 registers) unless a thread holds more than 16 points
+    static constexpr int kMinBlocks = T <= 256 ? (Q::N / T > 16 ? 2 : 3) : 1;
     template <bool FWD, class Src0, class DstL>
     __device__ __forceinline__ static void run(const TileDesc &d, float2 *work, const Src0 &src0, const DstL &dstL,
                                                bool dst_in_place, int lane, bool active)

@@ -78,6 +78,8 @@ __device__ __forceinline__ void load_tile(const TileDesc &d, const void *in, flo
                     } else {
                         v = cconj(x[nb - e]);
                     }
+                } else if (d.planar & 1) {
+                    v = make_float2(static_cast<const float *>(in)[base + e], d.in_im[base + e]);
                 } else {
                     v = static_cast<const float2 *>(in)[base + e];
                 }
@@ -116,6 +118,19 @@ __device__ __forceinline__ void load_tile(const TileDesc &d, const void *in, flo
     const int64_t base = col_base(d.in_a, o, c0 + l);
     const int64_t es = d.in_a.estride;
     float2 *row = sm + l * P;
+    if (d.planar & 1) {
+        // separated real / imaginary planes (C2C)
+        const float *xr = static_cast<const float *>(in) + base;
+        const float *xi = d.in_im + base;
+        if (d.g_twiddle) {
+            const int64_t kc = (c0 + l) % d.g_ns;
+            for (int e = e0; e < n; e += estep)
+                row[pad(e)] = cmul(make_float2(xr[e * es], xi[e * es]), pass_twiddle<FWD>(d, e, kc));
+        } else {
+            for (int e = e0; e < n; e += estep) row[pad(e)] = make_float2(xr[e * es], xi[e * es]);
+        }
+        return;
+    }
     if (io == IO_R2C_FULL) {
         const float *x = static_cast<const float *>(in) + base;
         for (int e = e0; e < n; e += estep) row[pad(e)] = make_float2(x[e * es], 0.f);
@@ -166,6 +181,14 @@ __device__ __forceinline__ void store_tile(const TileDesc &d, void *out, const f
         } else if (d.blue_kind == 2) {
             float *y = static_cast<float *>(out) + base;
             for (int e = lane; e < d.blue_n; e += d.tpt) y[e] = cmul(row[pad(e)], __ldg(d.chirp + e)).x;
+        } else if (d.planar & 2) {
+            float *yr = static_cast<float *>(out) + base;
+            float *yi = d.out_im + base;
+            for (int e = lane; e < d.blue_n; e += d.tpt) {
+                const float2 v = cmul(row[pad(e)], __ldg(d.chirp + e));
+                yr[e] = v.x;
+                yi[e] = v.y;
+            }
         } else {
             const int count = d.blue_kind == 1 ? d.blue_n / 2 + 1 : d.blue_n;
             float2 *y = static_cast<float2 *>(out) + base;
@@ -188,6 +211,16 @@ __device__ __forceinline__ void store_tile(const TileDesc &d, void *out, const f
     const int64_t base = col_base(d.out_a, o, c0 + l);
     const int64_t es = d.out_a.estride;
     const float2 *row = sm + l * P;
+    if (d.planar & 2) {
+        float *yr = static_cast<float *>(out) + base;
+        float *yi = d.out_im + base;
+        for (int e = e0; e < n; e += estep) {
+            const float2 v = row[pad(e)];
+            yr[e * es] = v.x;
+            yi[e * es] = v.y;
+        }
+        return;
+    }
     if (io == IO_C2R_FULL) {
         float *y = static_cast<float *>(out) + base;
         for (int e = e0; e < n; e += estep) y[e * es] = row[pad(e)].x;

@@ -86,3 +86,20 @@ def test_reference_matrices_live(n):
         assert oracle.rel_l2(oracle.ref_dense("r2c", xr, n, fwd), oracle.r2c(xr, fwd)) < 1e-6
         xh = (rng.standard_normal((2, n // 2 + 1)) + 1j * rng.standard_normal((2, n // 2 + 1))).astype(np.complex64)
         assert oracle.rel_l2(oracle.ref_dense("c2r", xh, n, fwd), oracle.c2r(xh, n, fwd)) < 1e-6
+
+
+def test_istft_oracle_matches_torch_istft():
+    """The ISTFT restatement (reference center / normalized / onesided /
+    return_complex limits) equals torch.istft, whose semantics the reference
+    ports, for even and odd n_fft and hop < n_fft."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    for n_fft, hop, frames, ch in [(64, 16, 10, 2), (400, 160, 7, 3), (255, 100, 5, 1), (1024, 256, 9, 2)]:
+        x = rng.standard_normal((ch, n_fft, frames)) + 1j * rng.standard_normal((ch, n_fft, frames))
+        w = np.hanning(n_fft) + 0.1
+        a = oracle.istft(x, n_fft, hop, w)
+        b = torch.istft(torch.from_numpy(x), n_fft, hop, n_fft, torch.from_numpy(w), center=True,
+                        normalized=False, onesided=False, return_complex=True).numpy()
+        assert a.shape == b.shape == (ch, n_fft + hop * (frames - 1) - 2 * (n_fft // 2))
+        assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
