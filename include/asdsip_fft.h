@@ -144,7 +144,10 @@ ASDSIP_API AspbStatus asdFftMakePlan1D(asdFftHandle handle, int64_t fftSize, enu
                             enum asdFftDirection direction, int64_t batchSize,
                             enum asdFft1dDimType dimType ASDSIP_DEFAULT(ASCEND_FFT_HORIZONTAL));
 
-/* ISTFT plan.  (fft_api.h:59-62; core/fft/istft.cpp:495-575) */
+/* ISTFT plan for input complex64 [channel, nFft, frames] (frames > 1, 0 < hop <= winLength == nFft < 1500,
+ * hop < 1500); center / normalized / onesided / length / returnComplex are forced to true / false / false / 0 /
+ * true as in the reference.  Builds an INVERSE C2C plan (GetType reports C2C) that needs a workspace.
+ * (fft_api.h:59-62; core/fft/istft.cpp:300-390, 530-552) */
 ASDSIP_API AspbStatus asdFftIstftMakePlan(asdFftHandle handle, const aclTensor *input, const int64_t nFft,
                                const int64_t hopLengthOpt, const int64_t winLengthOpt,
                                const bool center ASDSIP_DEFAULT(true), const bool normalized ASDSIP_DEFAULT(false),
@@ -154,7 +157,9 @@ ASDSIP_API AspbStatus asdFftIstftMakePlan(asdFftHandle handle, const aclTensor *
 /* C2C on complex64 tensors whose trailing dims equal the plan sizes.  (fft_api.h:65; fft_api.cpp:1169-1189) */
 ASDSIP_API AspbStatus asdFftExecC2C(asdFftHandle handle, const aclTensor *input, const aclTensor *output);
 
-/* C2C on planar float32 real/imag tensors (plan type ASCEND_FFT_C2C_SEP).  (fft_api.h:68-69; fft_api.cpp:1284-1342) */
+/* C2C on planar float32 real/imag tensors of a plan made with type ASCEND_FFT_C2C_SEP (1D, 2D or 3D); the four
+ * tensors must have the same shape (else ACL_ERROR_INTERNAL_ERROR, as in the reference); in place when both
+ * planes are.  (fft_api.h:68-69; fft_api.cpp:1236-1342) */
 ASDSIP_API AspbStatus asdFftExecC2CSeparated(asdFftHandle handle, const aclTensor *inputReal, const aclTensor *inputImag,
                                   const aclTensor *outputReal, const aclTensor *outputImag);
 
@@ -164,7 +169,8 @@ ASDSIP_API AspbStatus asdFftExecC2R(asdFftHandle handle, const aclTensor *input,
 /* R2C: float32 [.., N] -> complex64 [.., N/2+1].  (fft_api.h:76; fft_api.cpp:1213-1233) */
 ASDSIP_API AspbStatus asdFftExecR2C(asdFftHandle handle, const aclTensor *input, const aclTensor *output);
 
-/* ISTFT execution.  (fft_api.h:78-79; core/fft/istft.cpp) */
+/* ISTFT execution: window float32 [nFft], output complex64 [channel, nFft + hop (frames - 1) - 2 (nFft / 2)].
+ * (fft_api.h:78-79; core/fft/istft.cpp:554-575; fftcore/fft_core_istft_any.cpp:292-378) */
 ASDSIP_API AspbStatus asdFftExecIstft(asdFftHandle handle, const aclTensor *input, const aclTensor *windowOpt,
                            const aclTensor *output);
 
