@@ -482,7 +482,10 @@ def run_serving(args, world, rank, local):
         keep += [xt, ot]
         pin.append(xt.data_ptr())
         pout.append(ot.data_ptr())
-    srv = fft.Server(budget_bytes=32 << 30, lanes=args.lanes, max_rows=rows_max, device_io=args.device_io)
+    precision = {"fp32": fft.PRECISION_FP32, "fp16x3": fft.PRECISION_FP16X3,
+                 "bf16x3": fft.PRECISION_BF16X3}[args.precision]
+    srv = fft.Server(budget_bytes=32 << 30, lanes=args.lanes, max_rows=rows_max, device_io=args.device_io,
+                     precision=precision)
     for t, n in classes:
         srv.warm(t, fft.ASCEND_FFT_FORWARD, n)
     # warm-up traffic: allocates each lane's staging buffers
@@ -507,7 +510,9 @@ def run_serving(args, world, rank, local):
     if rank == 0:
         print(json.dumps({
             "metric": "serving p50/p99 latency (ms) and throughput vs offered load", "unit": "ms",
-            "form": "plain FP32", "io": "device-resident buffers" if args.device_io else "pinned host buffers",
+            "form": {"fp32": "plain FP32", "fp16x3": "split FP16 hi/lo x3 (tensor-core stages where available)",
+                     "bf16x3": "split BF16 hi/lo x3 (tensor-core stages where available)"}[args.precision],
+            "io": "device-resident buffers" if args.device_io else "pinned host buffers",
             "config": {"workload": "Poisson arrivals; R2C or C2C FP32, N in {4096, 8192, 16384, 65536}, rows "
                                    "uniform in [64, 1024], chirp + noise at SNR U[0,20] dB; 32 GiB admission budget",
                        "lanes": args.lanes, "max_rows": rows_max},
@@ -603,7 +608,7 @@ def main():
     ap.add_argument("--check", action="store_true", help="(kernel) check one transform against the oracle")
     ap.add_argument("--reps", type=int, default=20, help="(kernel) executions per timed sample")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16x3", "bf16x3"],
-                    help="(kernel) stage arithmetic: FP32 kernels or tensor-core hi/lo split forms")
+                    help="(kernel, serving) stage arithmetic: FP32 kernels or tensor-core hi/lo split forms")
     ap.add_argument("--device-io", action="store_true", help="(serving) request buffers in HBM instead of pinned host")
     ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--rates", default="1,10,100,1000,10000,50000")

@@ -66,6 +66,9 @@ ASDSIP_API int32_t asdFftTuneCacheLoad(const char *cache_path);
  * batched into one launch.  device_io != 0: request buffers are device pointers, else host (pinned). */
 ASDSIP_API int32_t asdFftServerCreate(void **server, int64_t budget_bytes, int32_t lanes, int64_t max_rows,
                                       int32_t device_io);
+/* Stage arithmetic of the server's resident plans (modes of asdFftSetPrecision); call before the first
+ * Warm / Submit (ACL_ERROR_INVALID_PARAM afterwards). */
+ASDSIP_API int32_t asdFftServerSetPrecision(void *server, int32_t mode);
 ASDSIP_API int32_t asdFftServerWarm(void *server, int32_t type, int32_t direction, int64_t n);
 /* Returns the request id (>= 0) or -1. */
 ASDSIP_API int64_t asdFftServerSubmit(void *server, int32_t type, int32_t direction, int64_t n, int64_t rows,

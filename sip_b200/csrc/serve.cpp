@@ -156,6 +156,16 @@ public:
         return out;
     }
 
+    // Arithmetic of the resident plans (asdFftSetPrecision modes); only
+    // before the first plan exists, so every request class uses one form.
+    bool set_precision(int mode)
+    {
+        std::lock_guard<std::mutex> lock(plan_mu_);
+        if (!plans_.empty()) return false;
+        precision_ = mode;
+        return true;
+    }
+
     int64_t batches() const { return batches_.load(); }
     int64_t failures() const { return failures_.load(); }
 
@@ -172,6 +182,7 @@ private:
         p->strides = {1};
         p->batch = max_rows_;
         p->device = device_;
+        p->precision = precision_;
         std::string e = build_plan_1d(*p);
         if (!e.empty()) {
             last_err_ = e;
@@ -334,6 +345,7 @@ private:
     int device_;
     std::vector<Lane> lanes_;
     std::map<std::tuple<int, int, int64_t>, std::unique_ptr<Plan>> plans_;
+    int precision_ = 0;
     std::mutex plan_mu_;
     std::string last_err_;
     std::mutex mu_;
@@ -390,6 +402,13 @@ int32_t asdFftServerCreate(void **server, int64_t budget_bytes, int32_t lanes, i
     } catch (...) {
         return AsdSip::ACL_ERROR_INTERNAL_ERROR;
     }
+}
+
+int32_t asdFftServerSetPrecision(void *server, int32_t mode)
+{
+    sipfft::Server *s = find_server(server);
+    if (!s || mode < 0 || mode > 2) return AsdSip::ACL_ERROR_INVALID_PARAM;
+    return s->set_precision(mode) ? AsdSip::ACL_SUCCESS : AsdSip::ACL_ERROR_INVALID_PARAM;
 }
 
 int32_t asdFftServerWarm(void *server, int32_t type, int32_t direction, int64_t n)

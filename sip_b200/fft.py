@@ -65,7 +65,7 @@ EXPORTED_SYMBOLS = (
     "asdFftBatchDescribe", "asdFftAutotune", "asdFftTuneCacheLoad",
     "asdFftServerCreate", "asdFftServerWarm", "asdFftServerSubmit", "asdFftServerDrain", "asdFftServerBatches",
     "asdFftServerDestroy", "asdFftServeRun", "asdFftServerHold", "asdFftGetErrorMessage",
-    "asdFftExecC2CNoAlloc", "asdFftSetPrecision",
+    "asdFftExecC2CNoAlloc", "asdFftSetPrecision", "asdFftServerSetPrecision",
 )
 
 
@@ -128,6 +128,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "asdFftDescribePlan": (i64, [vp, ctypes.c_char_p, i64]),
         "asdFftPlanLaunchCount": (i32, [vp]),
         "asdFftSetPrecision": (i32, [vp, i32]),
+        "asdFftServerSetPrecision": (i32, [vp, i32]),
         "asdFftBatchPlanCreate": (i32, [ctypes.POINTER(vp), P64, P64, i32, i32, ctypes.c_char_p]),
         "asdFftBatchGetWorkspaceSize": (i32, [vp, ctypes.POINTER(sz)]),
         "asdFftBatchExec": (i32, [vp, vp, vp, vp, vp, i32]),
@@ -433,13 +434,18 @@ def tune_cache_load(cache_path: str) -> int:
 class Server:
     """The library's C++ continuous-batching FFT server (see include/asdsip_fft_ext.h)."""
 
-    def __init__(self, budget_bytes=32 << 30, lanes=4, max_rows=1024, device_io=False):
+    def __init__(self, budget_bytes=32 << 30, lanes=4, max_rows=1024, device_io=False,
+                 precision: int = PRECISION_FP32):
         h = ctypes.c_void_p()
         st = load_library().asdFftServerCreate(ctypes.byref(h), int(budget_bytes), int(lanes), int(max_rows),
                                                1 if device_io else 0)
         if st != ACL_SUCCESS:
             raise FftError("asdFftServerCreate", st)
         self.handle = h.value
+        if precision != PRECISION_FP32:
+            st = load_library().asdFftServerSetPrecision(self.handle, int(precision))
+            if st != ACL_SUCCESS:
+                raise FftError("asdFftServerSetPrecision", st)
 
     def warm(self, fft_type, direction, n):
         return load_library().asdFftServerWarm(self.handle, fft_type, direction, n)

@@ -102,3 +102,30 @@ def test_server_rejects_bad_requests(cuda):
     ids, _ = srv.drain()
     assert len(ids) == 0
     srv.close()
+
+
+@pytest.mark.parametrize("precision", [fft.PRECISION_FP16X3, fft.PRECISION_BF16X3], ids=["fp16x3", "bf16x3"])
+def test_split_precision_server(cuda, precision):
+    """A server whose resident plans use the tensor-core split forms: results within the
+    FP32 bar for every class (C2C 4096 takes the tensor-core row pipeline, R2C 8192 the
+    tensor-core tile kernel, the other classes the FP32 kernels); the precision cannot be
+    changed once plans exist."""
+    import torch
+
+    srv = fft.Server(budget_bytes=8 << 30, lanes=2, max_rows=256, device_io=True, precision=precision)
+    assert fft.load_library().asdFftServerSetPrecision(srv.handle, fft.PRECISION_FP32) == fft.ACL_SUCCESS
+    assert fft.load_library().asdFftServerSetPrecision(srv.handle, precision) == fft.ACL_SUCCESS
+    work = []
+    for i, (typ, n) in enumerate([(C2C, 4096), (R2C, 8192), (C2C, 16384), (R2C, 4096), (C2C, 4096)]):
+        rows = 37 + 11 * i
+        x, xin, out = _host_buffers(torch, typ, n, rows, seed=700 + i)
+        xin, out = xin.cuda(), out.cuda()
+        work.append((typ, n, x, xin, out))
+        assert srv.submit(typ, FWD, n, rows, xin.data_ptr(), out.data_ptr()) >= 0
+    ids, lat = srv.drain()
+    assert len(ids) == 5 and np.all(lat > 0)
+    torch.cuda.synchronize()
+    for typ, n, x, _, out in work:
+        assert oracle.rel_l2(out.cpu().numpy(), _ref(typ, x)) <= oracle.tolerance(n)
+    assert fft.load_library().asdFftServerSetPrecision(srv.handle, fft.PRECISION_FP32) == fft.ACL_ERROR_INVALID_PARAM
+    srv.close()
