@@ -171,9 +171,11 @@ std::vector<TuneChoice> tune_candidates(int64_t n)
         }
         if (t == 2) r8.push_back(4);
         if (t == 1) r8.push_back(2);
-        for (int x : base)
-            if (x % 2) r8.push_back(x);
-        orders.push_back(r8);
+        std::vector<int> odd;
+        if (factor_radices(m, odd)) {  // m is odd: only odd radices
+            for (int x : odd) r8.push_back(x);
+            orders.push_back(r8);
+        }
         std::vector<int> oddfirst;
         for (int x : base)
             if (x % 2) oddfirst.push_back(x);

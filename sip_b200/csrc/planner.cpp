@@ -29,7 +29,7 @@ constexpr int kRowThreadsTarget = 256;     // threads per CTA for batched rows
 constexpr int kRowSmemTarget = 64 * 1024;  // keep >= 3 CTAs per SM for short rows
 constexpr int kColTile = 16;               // columns per tile: 16 x 8 B = one 128-byte line
 constexpr int kMaxThreads = 512;           // launch bound of the tile kernel (keeps 128 registers/thread)
-const int kRadices[] = {16, 13, 11, 8, 7, 5, 4, 3, 2};
+const int kRadices[] = {16, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2};
 
 int padded(int i) { return i + (i >> 4); }
 
@@ -699,7 +699,7 @@ bool valid_radices(const std::vector<int> &r, int64_t n)
 {
     int64_t prod = 1;
     for (int x : r) {
-        if (x != 2 && x != 3 && x != 4 && x != 5 && x != 7 && x != 8 && x != 11 && x != 13 && x != 16) return false;
+        if (x < 2 || x > 16 || x == 14 || x == 15) return false;
         prod *= x;
     }
     return prod == n && r.size() <= static_cast<size_t>(kMaxStages);
@@ -720,12 +720,36 @@ bool factor_radices(int64_t n, std::vector<int> &radices)
         const int base = twos / s, extra = twos % s;
         for (int i = 0; i < s; i++) radices.push_back(1 << (base + (i < extra ? 1 : 0)));
     }
-    for (int p : {13, 11, 7, 5, 3}) {
+    // odd part: pairs of 3 as radix 9, then the primes
+    std::vector<int> odd;
+    for (int p : {13, 11, 7, 5}) {
         while (m % p == 0) {
-            radices.push_back(p);
+            odd.push_back(p);
             m /= p;
         }
     }
+    while (m % 9 == 0) {
+        odd.push_back(9);
+        m /= 9;
+    }
+    if (m % 3 == 0) {
+        // a single 3 (or a 5 below) joins a power-of-two radix when that keeps it <= 16: 4*3, 2*3, 2*5
+        m /= 3;
+        auto it = std::find(radices.begin(), radices.end(), 4);
+        if (it == radices.end()) it = std::find(radices.begin(), radices.end(), 2);
+        if (it != radices.end()) *it *= 3;
+        else odd.push_back(3);
+    }
+    for (int &r : odd) {
+        if (r != 5) continue;
+        auto it = std::find(radices.begin(), radices.end(), 2);
+        if (it != radices.end()) {
+            *it = 10;
+            r = 1;
+        }
+    }
+    for (int r : odd)
+        if (r > 1) radices.push_back(r);
     return m == 1;
 }
 

@@ -30,7 +30,7 @@ constexpr int nb_for() { return (MAXE + R - 1) / R; }
 template <int MAXE>
 constexpr int maxv_for()
 {
-    constexpr int r[] = {2, 3, 4, 5, 7, 8, 11, 13, 16};
+    constexpr int r[] = {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 16};
     int m = 0;
     for (int x : r) m = m > ((MAXE + x - 1) / x) * x ? m : ((MAXE + x - 1) / x) * x;
     return m;
@@ -98,7 +98,7 @@ __device__ __forceinline__ void stage_scatter(const float2 *v, const Dst &dst, i
     }
 }
 
-#define SIPFFT_RADIX_CASES(X) X(2) X(3) X(4) X(5) X(7) X(8) X(11) X(13) X(16)
+#define SIPFFT_RADIX_CASES(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(16)
 
 template <int MAXE, bool FWD, class Src>
 __device__ __forceinline__ void gather_any(int R, float2 *v, const Src &src, int n, int ns, uint32_t nsm, int ts,

@@ -13,7 +13,9 @@ import numpy as np
 
 
 def factor_radices(n: int) -> list[int]:
-    """Same decomposition as planner.cpp factor_radices()."""
+    """Same decomposition as planner.cpp factor_radices(): powers of two in balanced
+    stages of <= 16, odd primes with pairs of 3 as 9, a single 3 or 5 merged into a
+    power-of-two radix (12, 6, 10) when there is one."""
     m, twos = n, 0
     while m % 2 == 0:
         m //= 2
@@ -23,10 +25,27 @@ def factor_radices(n: int) -> list[int]:
         s = (twos + 3) // 4
         base, extra = divmod(twos, s)
         out += [1 << (base + (1 if i < extra else 0)) for i in range(s)]
-    for p in (13, 11, 7, 5, 3):
+    odd = []
+    for p in (13, 11, 7, 5):
         while m % p == 0:
-            out.append(p)
+            odd.append(p)
             m //= p
+    while m % 9 == 0:
+        odd.append(9)
+        m //= 9
+    if m % 3 == 0:  # a single 3 joins a radix 4 (-> 12) or 2 (-> 6)
+        m //= 3
+        for want in (4, 2):
+            if want in out:
+                out[out.index(want)] *= 3
+                break
+        else:
+            odd.append(3)
+    for i, r in enumerate(odd):  # a 5 joins a radix 2 (-> 10)
+        if r == 5 and 2 in out:
+            out[out.index(2)] = 10
+            odd[i] = 1
+    out += [r for r in odd if r > 1]
     if m != 1:
         raise ValueError(f"{n} has a prime factor above 13")
     return out

@@ -8,8 +8,8 @@ import stockham_model as sm
 from oracle import oracle
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 7, 8, 11, 12, 13, 16, 30, 60, 64, 96, 100, 128, 143, 210,
-                               256, 343, 1000, 1024, 1500, 2048, 3000, 4096])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 16, 20, 27, 30, 60, 64, 81, 96, 100, 128,
+                               143, 210, 216, 245, 256, 343, 360, 1000, 1024, 1500, 2048, 3000, 4096])
 @pytest.mark.parametrize("fwd", [True, False])
 def test_smem_stockham(n, fwd):
     rng = np.random.default_rng(n)
