@@ -193,38 +193,6 @@ __global__ void __launch_bounds__(512, 1) tile_fft_kernel(const __grid_constant_
 // multi-pass steps): while a tile runs its stages, the element copies of the
 // CTA's next tile are already in flight into the second buffer (cp.async,
 // 8 bytes per element, no registers held), so HBM latency overlaps compute.
-__device__ __forceinline__ void cp_async8(void *dst, const void *src)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-__device__ __forceinline__ void issue_tile_c2c(const TileDesc &d, const void *in, float2 *sm, int64_t g)
-{
-    const int tid = threadIdx.x, bd = blockDim.x;
-    const int64_t o = g / d.tiles_per_outer;
-    const int64_t c0 = (g % d.tiles_per_outer) * d.tb;
-    const int64_t left = d.n_cols - c0;
-    const int ntr = left < d.tb ? static_cast<int>(left) : d.tb;
-    int l, e0, estep;
-    if (d.in_a.estride == 1) {
-        l = tid / d.tpt;
-        e0 = tid % d.tpt;
-        estep = d.tpt;
-    } else {
-        l = tid % d.tb;
-        e0 = tid / d.tb;
-        estep = bd / d.tb;
-    }
-    if (l >= ntr) return;
-    const float2 *x = static_cast<const float2 *>(in) + col_base(d.in_a, o, c0 + l);
-    const int64_t es = d.in_a.estride;
-    float2 *row = sm + l * d.pitch;
-    for (int e = e0; e < d.n; e += estep) cp_async8(row + pad(e), x + e * es);
-}
-
 template <int MAXE, bool FWD>
 __global__ void __launch_bounds__(512, 1) tile_db_kernel(const __grid_constant__ TileDesc d)
 {

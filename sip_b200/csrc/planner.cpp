@@ -217,6 +217,7 @@ struct Builder {
             s.has_row = false;
             s.row_fn = nullptr;
             s.db = false;
+            s.db_fn = nullptr;
             s.tc_fmt = -1;
             s.what += " [separated re/im]";
         }
@@ -287,11 +288,27 @@ struct Builder {
             (io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
             add_row_variant(s, c, ia.cstride, oa.cstride);
         if (column && io == IO_C2C && 2 * int64_t(d.tb) * d.pitch * 8 <= kMaxSmemBytes) {
-            // strided C2C axis or multi-pass step: double-buffered persistent tiles
+            // strided C2C axis or multi-pass step: double-buffered persistent tiles,
+            // with the compile-time engine of the length when one matches the tile shape
             const size_t smem = 2 * size_t(d.tb) * d.pitch * 8;
-            const int per_sm = kernel_blocks_per_sm(tile_db_kernel_fn(s.maxe, s.forward), d.tb * d.tpt, smem);
+            const void *fn = tile_db_kernel_fn(s.maxe, s.forward);
+            const StaticKernel *sk = find_static_kernel(n, IO_C2C);
+            const float2 *stw = d.stw;
+            if (sk && sk->tpt == d.tpt && sk->db[s.forward ? 1 : 0]) {
+                TablePtr t = get_stage_table(*sk, device, &err);
+                if (!t) return false;
+                p.tables.push_back(t);
+                fn = sk->db[s.forward ? 1 : 0];
+                stw = t->ptr;
+            }
+            const int per_sm = kernel_blocks_per_sm(fn, d.tb * d.tpt, smem);
             if (per_sm > 0) {
                 s.db = true;
+                if (fn != tile_db_kernel_fn(s.maxe, s.forward)) {
+                    // d keeps the runtime radices' tables; the engine's own go in db_stw
+                    s.db_fn = fn;
+                    s.db_stw = stw;
+                }
                 s.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(d.num_tiles, int64_t(per_sm) * sm_count(device))));
             }
         }
@@ -863,7 +880,8 @@ std::string describe_plan(const Plan &p)
     for (const Step &s : p.steps) {
         o << "  [" << static_cast<int>(s.src) << "->" << static_cast<int>(s.dst) << "] " << s.what;
         if (s.kind == StepKind::kTile) {
-            o << (s.db ? " [double-buffered]" : "") << " n=" << s.d.n << " radices=";
+            o << (s.db ? (s.db_fn ? " [double-buffered, static engine]" : " [double-buffered]") : "") << " n=" << s.d.n
+              << " radices=";
             for (int i = 0; i < s.d.nstages; i++) o << (i ? "x" : "") << s.d.radix[i];
             o << " tb=" << s.d.tb << " tpt=" << s.d.tpt << " tiles=" << s.d.num_tiles << " grid=" << s.grid
               << " smem=" << s.d.tb * s.d.pitch * 8;

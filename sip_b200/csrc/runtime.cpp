@@ -259,7 +259,13 @@ cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const v
                     TileDesc d = s.d;
                     d.in = src;
                     d.out = dst;
-                    e = launch_tile_db(d, s.maxe, s.forward, s.grid, st);
+                    if (s.db_fn) {
+                        d.stw = s.db_stw;
+                        e = launch_kernel_fn(s.db_fn, d, s.grid, 2 * size_t(d.tb) * d.pitch * sizeof(float2),
+                                             device_error_word(p.device), st);
+                    } else {
+                        e = launch_tile_db(d, s.maxe, s.forward, s.grid, st);
+                    }
                 } else {
                     TileDesc d = s.d;
                     d.in = src;

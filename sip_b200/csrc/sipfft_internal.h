@@ -61,6 +61,7 @@ struct StaticKernel {
     int radix[8] = {};
     int tpt = 0;
     const void *fn[2][3] = {};  // [forward][C2C, R2C packed, C2R packed]
+    const void *db[2] = {};     // [forward] double-buffered C2C tiles (strided axes, multi-pass steps)
 };
 const StaticKernel *find_static_kernel(int n, int io);
 cudaError_t fill_stage_twiddles(float2 *t, const int *radix, int nstages, cudaStream_t st);
@@ -144,6 +145,8 @@ struct Step {
     // source pointer is 16-byte aligned); row_fn != nullptr selects a
     // compile-time specialised kernel instead of the runtime-radix one
     bool db = false;  // run d on the double-buffered tile kernel (grid is then persistent)
+    const void *db_fn = nullptr;  // compile-time engine for it (else the runtime-radix kernel)
+    const float2 *db_stw = nullptr;  // that engine's per-stage twiddle tables
     bool has_row = false;
     TileDesc rd{};
     int row_grid = 1;

@@ -8,6 +8,7 @@
 // engines plug into the TMA-pipelined row skeleton (pipelined_rows.cuh).
 // Lengths without a specialisation use the runtime-radix engine.
 #include "pipelined_rows.cuh"
+#include "tile_io.cuh"
 
 namespace sipfft {
 
@@ -229,6 +230,60 @@ struct StaticEngine {
     }
 };
 
+// ------------------------------------------------------------------------------------ double-buffered tiles
+// The engines in the double-buffered tile skeleton (strided axes and
+// multi-pass steps): the next tile's element copies are in flight (cp.async)
+// while the engine runs the current tile in place; the first stage applies the
+// inter-pass twiddles of a multi-pass step on read.
+template <bool FWD>
+struct PassRow {
+    const float2 *row;
+    const TileDesc *d;
+    int64_t kc;
+    __device__ __forceinline__ float2 operator()(int e) const
+    {
+        return cmul(row[pad(e)], pass_twiddle<FWD>(*d, e, kc));
+    }
+};
+
+template <class E, bool FWD>
+__global__ void __launch_bounds__(512, 1) static_db_kernel(const __grid_constant__ TileDesc d, int *)
+{
+    extern __shared__ float2 sm[];
+    const int64_t span = int64_t(d.tb) * d.pitch;
+    const int tid = threadIdx.x;
+    const int l = d.xfast ? tid % d.tb : tid / d.tpt;
+    const int lane = d.xfast ? tid / d.tb : tid % d.tpt;
+    const bool thread_on = tid < d.tb * d.tpt;
+    int64_t g = blockIdx.x;
+    if (g < d.num_tiles) issue_tile_c2c(d, d.in, sm, g);
+    cp_async_commit();
+    for (int i = 0; g < d.num_tiles; g += gridDim.x, i++) {
+        float2 *cur = sm + (i & 1) * span;
+        const int64_t gn = g + gridDim.x;
+        if (gn < d.num_tiles) issue_tile_c2c(d, d.in, sm + ((i + 1) & 1) * span, gn);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        const int64_t o = g / d.tiles_per_outer;
+        const int64_t c0 = (g % d.tiles_per_outer) * d.tb;
+        const int64_t left = d.n_cols - c0;
+        const int ntr = left < d.tb ? static_cast<int>(left) : d.tb;
+        float2 *row = cur + (thread_on ? l : 0) * d.pitch;
+        const bool act = thread_on && l < ntr;
+        if (d.g_twiddle) {
+            const int64_t kc = (c0 + (thread_on ? l : 0)) % d.g_ns;
+            E::template run<FWD>(d, row, PassRow<FWD>{row, &d, kc}, SmemRow{row}, true, lane, act);
+        } else {
+            E::template run<FWD>(d, row, SmemRow{row}, SmemRow{row}, true, lane, act);
+        }
+        __syncthreads();
+        store_tile<FWD>(d, d.out, cur, o, c0, ntr);
+        __syncthreads();
+    }
+    cp_async_wait<0>();
+}
+
 // ------------------------------------------------------------------------------------ registry
 namespace {
 
@@ -248,6 +303,8 @@ StaticKernel make_entry(int io_mask = 7)
     e.fn[0][0] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, false, IO_C2C>);
     e.fn[0][1] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, false, IO_R2C_PACKED>);
     e.fn[0][2] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, false, IO_C2R_PACKED>);
+    e.db[1] = reinterpret_cast<const void *>(static_db_kernel<E, true>);
+    e.db[0] = reinterpret_cast<const void *>(static_db_kernel<E, false>);
     return e;
 }
 
@@ -272,8 +329,10 @@ const std::vector<StaticKernel> &registry()
 void static_kernel_fns(std::vector<const void *> &out)
 {
     for (const StaticKernel &e : registry())
-        for (int f = 0; f < 2; f++)
+        for (int f = 0; f < 2; f++) {
             for (int io = 0; io < 3; io++) out.push_back(e.fn[f][io]);
+            out.push_back(e.db[f]);
+        }
 }
 
 const StaticKernel *find_static_kernel(int n, int io)

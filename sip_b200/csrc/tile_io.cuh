@@ -3,6 +3,7 @@
 // Shared by the SIMT tile kernel (fft_tile.cu) and the tensor-core kernel
 // (tc_fft.cu).  The shared-memory row index is padded (pad(i) = i + i/16).
 #pragma once
+#include "async_copy.cuh"
 #include "codelets.cuh"
 #include "fft_tile.cuh"
 
@@ -230,6 +231,44 @@ __device__ __forceinline__ void store_tile(const TileDesc &d, void *out, const f
     float2 *y = static_cast<float2 *>(out) + base;
     for (int e = e0; e < count; e += estep) y[e * es] = row[pad(e)];
 }
+
+// ------------------------------------------------------------------------------------ async tile loads
+// Element copies of one C2C tile issued with cp.async (8 bytes per element, no
+// registers held); a double-buffered kernel issues the next tile's copies
+// before it runs the current one.  Inter-pass twiddles are left to the first
+// stage.
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void issue_tile_c2c(const TileDesc &d, const void *in, float2 *sm, int64_t g)
+{
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int64_t o = g / d.tiles_per_outer;
+    const int64_t c0 = (g % d.tiles_per_outer) * d.tb;
+    const int64_t left = d.n_cols - c0;
+    const int ntr = left < d.tb ? static_cast<int>(left) : d.tb;
+    int l, e0, estep;
+    if (d.in_a.estride == 1) {
+        l = tid / d.tpt;
+        e0 = tid % d.tpt;
+        estep = d.tpt;
+    } else {
+        l = tid % d.tb;
+        e0 = tid / d.tb;
+        estep = bd / d.tb;
+    }
+    if (l >= ntr) return;
+    const float2 *x = static_cast<const float2 *>(in) + col_base(d.in_a, o, c0 + l);
+    const int64_t es = d.in_a.estride;
+    float2 *row = sm + l * d.pitch;
+    for (int e = e0; e < d.n; e += estep) cp_async8(row + pad(e), x + e * es);
+}
+
 
 // One tile: load, Stockham stages, store.  Threads beyond tb*tpt (a launch
 // shared by tiles of different shapes) only take part in the barriers.
