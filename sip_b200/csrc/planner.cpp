@@ -24,6 +24,7 @@ bool valid_radices(const std::vector<int> &r, int64_t n);
 namespace {
 
 constexpr int64_t kMaxRowN = 16384;        // longest single-CTA transform: 512 threads x 32 points
+constexpr int64_t kMaxSingleTileC2C = 8192;  // longest C2C row planned as one tile
 constexpr int kMaxPassRadix = 2048;        // longest sub-FFT of one multi-pass Stockham pass
 constexpr int kRowThreadsTarget = 256;     // threads per CTA for batched rows
 constexpr int kRowSmemTarget = 64 * 1024;  // keep >= 3 CTAs per SM for short rows
@@ -571,7 +572,9 @@ struct Builder {
         const bool smooth = factor_radices(n, probe);
         if (inner == 1 && !smooth) return add_bluestein(0, n, outer, n, n, src, dst);
         if (inner == 1) {
-            if (n <= std::min<int64_t>(kMaxRowN, p.max_row_n)) {
+            // rows up to 8192 points run as one tile; longer rows as two double-buffered
+            // passes, which keep ~16 columns per tile and overlap loads with compute
+            if (n <= std::min<int64_t>(kMaxSingleTileC2C, p.max_row_n)) {
                 const float2 *tw = table(n, n);
                 if (!tw) return false;
                 Addr a{0, n, 1, 0, 0};
