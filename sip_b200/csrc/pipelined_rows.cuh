@@ -27,7 +27,9 @@ struct StageRow {
     __device__ __forceinline__ float2 operator()(int e) const { return row[e]; }
 };
 
-// C2R input seen as the packed m-point sequence Z (computed from X[e], X[m-e])
+// C2R input seen as the packed m-point sequence Z (computed from X[e], X[m-e]):
+// Z[e] = E + i O, E = X[e] + conj X[m-e], O = w^e (X[e] - conj X[m-e]),
+// w = exp(-+2 pi i / 2m); DC and Nyquist imaginary parts are ignored.
 template <bool FWD>
 struct C2RPre {
     const float2 *x;  // staged half spectrum, m+1 bins
@@ -41,32 +43,43 @@ struct C2RPre {
             xk.y = 0.f;
             xm.y = 0.f;
         }
-        const float2 ev = cadd(xk, cconj(xm));
-        const float2 od = cmul(csub(xk, cconj(xm)), dir<FWD>(__ldg(tw + e)));
+        const float2 ev = make_float2(xk.x + xm.x, xk.y - xm.y);
+        const float2 od = cmul(make_float2(xk.x - xm.x, xk.y + xm.y), dir<FWD>(__ldg(tw + e)));
         return make_float2(ev.x - od.y, ev.y + od.x);
     }
 };
+
+// R2C bins k and m-k from Z[k], Z[m-k] and w = w^k (direction applied):
+// X[k] = S/2 + w U/2 and X[m-k] = conj(S/2 - w U/2), with S = Z[k] + conj Z[m-k]
+// and U = -i (Z[k] - conj Z[m-k]).
+__device__ __forceinline__ void r2c_pair(float2 zk, float2 zm, float2 w, float2 &xk, float2 &xm)
+{
+    const float sx = zk.x + zm.x, sy = zk.y - zm.y;
+    const float2 u = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    const float2 wu = cmul(w, u);
+    xk = make_float2(fmaf(0.5f, sx, wu.x), fmaf(0.5f, sy, wu.y));
+    xm = make_float2(fmaf(0.5f, sx, -wu.x), fmaf(-0.5f, sy, wu.y));
+}
 
 struct GlobalRow {
     float2 *row;
     __device__ __forceinline__ void operator()(int e, float2 v) const { row[e] = v; }
 };
 
-// R2C post-twiddle from the padded work row to HBM: X[k] = E + w^k O,
-// X[n-k] = conj(E - w^k O) with E, O recovered from Z[k], conj(Z[n-k]).
+// R2C post-twiddle from the padded work row to HBM, one pair (k, n-k) per
+// iteration.
 template <bool FWD>
 __device__ __forceinline__ void r2c_post_row(const float2 *work, float2 *y, int n, int lane, int tpt,
-                                             const float2 *tw)
+                                             const float2 *__restrict__ tw)
 {
     for (int k = lane; 2 * k <= n; k += tpt) {
-        const float2 zk = work[pad(k)];
-        const float2 zm = cconj(work[pad(k == 0 ? 0 : n - k)]);
-        const float2 e = cscale(cadd(zk, zm), 0.5f);
-        const float2 tt = csub(zk, zm);
-        const float2 od = make_float2(0.5f * tt.y, -0.5f * tt.x);
-        const float2 wo = cmul(dir<FWD>(__ldg(tw + k)), od);
-        y[k] = cadd(e, wo);
-        if (2 * k != n) y[n - k] = cconj(csub(e, wo));
+        float2 a, b;
+        r2c_pair(work[pad(k)], work[pad(k == 0 ? 0 : n - k)], dir<FWD>(__ldg(tw + k)), a, b);
+        y[k] = a;
+        if (k == 0)
+            y[n] = b;
+        else if (2 * k != n)
+            y[n - k] = b;
     }
 }
 
@@ -115,19 +128,21 @@ __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
     }
     __syncthreads();
 
-    // Bytes of tile t that the bulk engine copies (a multiple of 16); a
-    // trailing 8-byte element, if any, is fetched with a plain load.
+    // Tile t spans elements [s, e) of the input.  The bulk engine copies the
+    // whole 16-byte lines [s & ~1, e & ~1) into the buffer, so with an odd
+    // s the staged rows start one element in (the copy's first element is the
+    // previous row's last); a trailing odd element is fetched with a plain load.
     auto tile_rows = [&](int64_t t) -> int {
         const int64_t left = rows_total - t * tb;
         return left < tb ? static_cast<int>(left) : tb;
     };
     auto issue = [&](int64_t t, int b) {
         if (tid == 0) {
-            const uint32_t bytes = static_cast<uint32_t>(tile_rows(t) * in_dist * 8);
-            const uint32_t bulk = bytes & ~15u;
+            const int64_t s = t * tb * in_dist, e = s + tile_rows(t) * in_dist;
+            const uint32_t bulk = static_cast<uint32_t>(((e & ~int64_t(1)) - (s & ~int64_t(1))) * 8);
             fence_proxy_async_smem();
             mbar_arrive_expect_tx(&bars[b], bulk);
-            if (bulk) bulk_g2s(bufs + b * buf_f2, in + t * tb * in_dist, bulk, &bars[b]);
+            if (bulk) bulk_g2s(bufs + b * buf_f2, in + (s & ~int64_t(1)), bulk, &bars[b]);
         }
     };
 
@@ -143,22 +158,23 @@ __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
         }
         const int rows = tile_rows(t);
         float2 *buf = bufs + b * buf_f2;
-        const int64_t bytes = rows * in_dist * 8;
-        if (bytes & 15) {  // uniform across the CTA
-            if (tid == 0) buf[rows * in_dist - 1] = in[t * tb * in_dist + rows * in_dist - 1];
+        const int64_t s = t * tb * in_dist, e = s + rows * in_dist;
+        const float2 *stage = buf + (s & 1);
+        if (e & 1) {  // uniform across the CTA
+            if (tid == 0) buf[(e - 1) - (s & ~int64_t(1))] = in[e - 1];
             __syncthreads();
         }
         const bool active = thread_on && l < rows;
         float2 *work = buf + l * d.pitch;
         const int64_t row_index = t * tb + l;
         if constexpr (IO == IO_C2C) {
-            Engine::template run<FWD>(d, work, StageRow{buf + l * in_dist}, GlobalRow{out + row_index * out_dist},
-                                      false, lane, active);
+            Engine::template run<FWD>(d, work, StageRow{stage + l * in_dist},
+                                      GlobalRow{out + row_index * out_dist}, false, lane, active);
         } else if constexpr (IO == IO_C2R_PACKED) {
-            Engine::template run<FWD>(d, work, C2RPre<FWD>{buf + l * in_dist, d.n, d.tw},
+            Engine::template run<FWD>(d, work, C2RPre<FWD>{stage + l * in_dist, d.n, d.tw},
                                       GlobalRow{out + row_index * out_dist}, false, lane, active);
         } else {  // IO_R2C_PACKED
-            Engine::template run_r2c<FWD>(d, work, StageRow{buf + l * in_dist}, out + row_index * out_dist, lane,
+            Engine::template run_r2c<FWD>(d, work, StageRow{stage + l * in_dist}, out + row_index * out_dist, lane,
                                           active);
         }
         __syncthreads();  // buffer b is free for the copy issued in iteration i+1

@@ -113,21 +113,6 @@ __device__ __forceinline__ void srun(float2 *v, float2 *work, const Src0 &src0, 
 // per SM (at most 85 registers per thread: the codelets fit without
 // spilling), which doubles the warps available to hide shared-memory and
 // twiddle-load latency compared with an unconstrained build.
-// R2C post-twiddle value for bin k from Z[k] and conj(Z[m-k]):
-// X[k] = E + w^k O, E = (Z[k] + conj Z[m-k]) / 2, O = -i (Z[k] - conj Z[m-k]) / 2.
-template <bool FWD>
-__device__ __forceinline__ float2 r2c_bin(float2 zk, float2 zmc, float2 w, float2 &e, float2 &wo)
-{
-    e = cscale(cadd(zk, zmc), 0.5f);
-    const float2 t = csub(zk, zmc);
-    wo = cmul(w, make_float2(0.5f * t.y, -0.5f * t.x));
-    return cadd(e, wo);
-}
-
-// Last stage of an R2C transform with the post-twiddle fused: the thread owns
-// butterflies j0 = lane and its mirror j1 = NBF - lane (lane 0: j1 = NBF/2),
-// so the partner Z[m-k] of every output k it produces is in its own
-// registers, and the N/2+1 bins are written straight to HBM.
 template <class Q, int T, bool FWD>
 struct FusedR2C {
     static constexpr int S = Q::S - 1;
@@ -153,21 +138,31 @@ struct FusedR2C {
             }
             dft<R, FWD>(v);
             dft<R, FWD>(v + R);
-            float2 e, wo;
+            float2 a, b;
             if (lane != 0) {
+                // bin j0 + r NBF pairs with its mirror j1 + (R-1-r) NBF
 #pragma unroll
                 for (int r = 0; r < R; r++) {
-                    const int k0 = j0 + r * NBF, k1 = j1 + r * NBF;
-                    y[k0] = r2c_bin<FWD>(v[r], cconj(v[R + R - 1 - r]), dir<FWD>(__ldg(tw + k0)), e, wo);
-                    y[k1] = r2c_bin<FWD>(v[R + r], cconj(v[R - 1 - r]), dir<FWD>(__ldg(tw + k1)), e, wo);
+                    const int k0 = j0 + r * NBF;
+                    r2c_pair(v[r], v[2 * R - 1 - r], dir<FWD>(__ldg(tw + k0)), a, b);
+                    y[k0] = a;
+                    y[j1 + (R - 1 - r) * NBF] = b;
                 }
             } else {
+                // bins r NBF pair with (R-r) NBF (r = 0: with the Nyquist bin N),
+                // bins NBF/2 + r NBF with NBF/2 + (R-1-r) NBF
 #pragma unroll
-                for (int r = 0; r < R; r++) {
-                    const int k0 = r * NBF, k1 = NBF / 2 + r * NBF;
-                    y[k0] = r2c_bin<FWD>(v[r], cconj(v[(R - r) % R]), dir<FWD>(__ldg(tw + k0)), e, wo);
-                    if (r == 0) y[N] = cconj(csub(e, wo));  // Nyquist bin from the k = 0 pair
-                    y[k1] = r2c_bin<FWD>(v[R + r], cconj(v[R + R - 1 - r]), dir<FWD>(__ldg(tw + k1)), e, wo);
+                for (int r = 0; 2 * r <= R; r++) {
+                    r2c_pair(v[r], v[(R - r) % R], dir<FWD>(__ldg(tw + r * NBF)), a, b);
+                    y[r * NBF] = a;
+                    if (2 * r != R) y[N - r * NBF] = b;
+                }
+#pragma unroll
+                for (int r = 0; 2 * r < R; r++) {
+                    const int k = NBF / 2 + r * NBF;
+                    r2c_pair(v[R + r], v[2 * R - 1 - r], dir<FWD>(__ldg(tw + k)), a, b);
+                    y[k] = a;
+                    if (2 * r != R - 1) y[N - k] = b;
                 }
             }
         }
