@@ -128,18 +128,22 @@ __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
     }
     __syncthreads();
 
-    // Tile t spans elements [s, e) of the input.  The bulk engine copies the
-    // whole 16-byte lines [s & ~1, e & ~1) into the buffer, so with an odd
-    // s the staged rows start one element in (the copy's first element is the
-    // previous row's last); a trailing odd element is fetched with a plain load.
+    // Tile t spans elements [s, e) of the input.  The bulk engine copies whole
+    // 16-byte lines from s & ~1, so with an odd s the staged rows start one
+    // element in (the copy's first element is the previous row's last); an odd
+    // e is rounded up (the next row's first element comes along) except at the
+    // end of the input, where the last element is fetched with a plain load.
+    // The input ends after the last row's own bins, not a full row distance on.
+    const int64_t total = (rows_total - 1) * in_dist + d.n + (IO == IO_C2R_PACKED ? 1 : 0);
     auto tile_rows = [&](int64_t t) -> int {
         const int64_t left = rows_total - t * tb;
         return left < tb ? static_cast<int>(left) : tb;
     };
     auto issue = [&](int64_t t, int b) {
         if (tid == 0) {
-            const int64_t s = t * tb * in_dist, e = s + tile_rows(t) * in_dist;
-            const uint32_t bulk = static_cast<uint32_t>(((e & ~int64_t(1)) - (s & ~int64_t(1))) * 8);
+            const int64_t s = t * tb * in_dist, e = min(s + tile_rows(t) * in_dist, total);
+            const int64_t z = e < total ? e + (e & 1) : e & ~int64_t(1);
+            const uint32_t bulk = static_cast<uint32_t>((z - (s & ~int64_t(1))) * 8);
             fence_proxy_async_smem();
             mbar_arrive_expect_tx(&bars[b], bulk);
             if (bulk) bulk_g2s(bufs + b * buf_f2, in + (s & ~int64_t(1)), bulk, &bars[b]);
@@ -158,9 +162,9 @@ __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
         }
         const int rows = tile_rows(t);
         float2 *buf = bufs + b * buf_f2;
-        const int64_t s = t * tb * in_dist, e = s + rows * in_dist;
+        const int64_t s = t * tb * in_dist, e = min(s + rows * in_dist, total);
         const float2 *stage = buf + (s & 1);
-        if (e & 1) {  // uniform across the CTA
+        if (e == total && (e & 1)) {  // last tile of an odd-length input; uniform across the CTA
             if (tid == 0) buf[(e - 1) - (s & ~int64_t(1))] = in[e - 1];
             __syncthreads();
         }

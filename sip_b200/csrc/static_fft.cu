@@ -314,7 +314,12 @@ const std::vector<StaticKernel> &registry()
         make_entry<Seq<16, 16, 8>, 128>(),      // 2048
         make_entry<Seq<16, 16, 16>, 256>(),     // 4096
         make_entry<Seq<16, 16, 16, 2>, 512>(),  // 8192
-        make_entry<Seq<10, 10, 15>, 100>(),     // 1500 (packed half of the 3000-point real transform)
+        // 1500, the packed half of the 3000-point real transform: R2C on a
+        // radix-5 last stage of 300 butterflies, two per thread, so that the
+        // post-twiddle fuses into it; C2C and C2R on 10 x 10 x 15, one
+        // butterfly per thread in the radix-10 stages
+        make_entry<Seq<12, 5, 5, 5>, 150>(4),
+        make_entry<Seq<10, 10, 15>, 150>(3),
     };
     return r;
 }
