@@ -43,8 +43,25 @@ struct C2RPre {
             xk.y = 0.f;
             xm.y = 0.f;
         }
+        return z(xk, xm, __ldg(tw + e));
+    }
+    // the same for e = j + off, twiddle w^j w^off
+    __device__ __forceinline__ float2 split(int j, int off) const
+    {
+        const int e = j + off;
+        float2 xk = x[e];
+        float2 xm = x[m - e];
+        if (e == 0) {
+            xk.y = 0.f;
+            xm.y = 0.f;
+        }
+        const float2 wj = __ldg(tw + j);
+        return z(xk, xm, off == 0 ? wj : cmul(wj, __ldg(tw + off)));
+    }
+    __device__ __forceinline__ static float2 z(float2 xk, float2 xm, float2 w)
+    {
         const float2 ev = make_float2(xk.x + xm.x, xk.y - xm.y);
-        const float2 od = cmul(make_float2(xk.x - xm.x, xk.y + xm.y), dir<FWD>(__ldg(tw + e)));
+        const float2 od = cmul(make_float2(xk.x - xm.x, xk.y + xm.y), dir<FWD>(w));
         return make_float2(ev.x - od.y, ev.y + od.x);
     }
 };
@@ -92,6 +109,12 @@ struct RuntimeEngine {
                                                bool dst_in_place, int lane, bool active)
     {
         run_fft<MAXE, FWD>(d, work, src0, true, dstL, dst_in_place, lane, active);
+    }
+    template <bool FWD, class DstL>
+    __device__ __forceinline__ static void run_c2r(const TileDesc &d, float2 *work, const float2 *x, const DstL &dstL,
+                                                   int lane, bool active)
+    {
+        run_fft<MAXE, FWD>(d, work, C2RPre<FWD>{x, d.n, d.tw}, true, dstL, false, lane, active);
     }
     // R2C: packed FFT into the work row, then the post-twiddle pass to HBM
     template <bool FWD, class Src0>
@@ -175,8 +198,8 @@ __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
             Engine::template run<FWD>(d, work, StageRow{stage + l * in_dist},
                                       GlobalRow{out + row_index * out_dist}, false, lane, active);
         } else if constexpr (IO == IO_C2R_PACKED) {
-            Engine::template run<FWD>(d, work, C2RPre<FWD>{stage + l * in_dist, d.n, d.tw},
-                                      GlobalRow{out + row_index * out_dist}, false, lane, active);
+            Engine::template run_c2r<FWD>(d, work, stage + l * in_dist, GlobalRow{out + row_index * out_dist}, lane,
+                                          active);
         } else {  // IO_R2C_PACKED
             Engine::template run_r2c<FWD>(d, work, StageRow{stage + l * in_dist}, out + row_index * out_dist, lane,
                                           active);

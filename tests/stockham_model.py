@@ -150,3 +150,101 @@ def c2r_packed(xh: np.ndarray, n: int, forward: bool) -> np.ndarray:
     out[0::2] = y.real
     out[1::2] = y.imag
     return out
+
+
+def fused_c2r_first_stage(xh: np.ndarray, m: int, R: int, forward: bool) -> np.ndarray:
+    """static_fft.cu FusedC2R::gather: thread `lane` (NBF/2 threads, NBF = m/R)
+    owns butterflies j0 = lane and j1 = NBF - lane (lane 0: 0 and NBF/2) and
+    builds their packed inputs Z[j + r NBF] pairwise; lane 0 runs the common
+    loop with selected inputs and twiddles, then moves its results into
+    butterfly order.  Returns Z (length m) assembled from every thread's
+    registers."""
+    nbf = m // R
+    G = (R + 1) // 2
+    w = np.exp((-1 if forward else 1) * 2j * np.pi * np.arange(m + 1) / (2 * m))
+
+    def pair(xk, xm, tw):
+        ev = xk + np.conj(xm)
+        od = (xk - np.conj(xm)) * tw
+        return ev + 1j * od, np.conj(ev) + 1j * np.conj(od)
+
+    def lane0_slot(k):
+        if k >= R:
+            return k - R if k - R < G else k
+        return G - 1 + k if k <= R - G else R - G + k
+
+    Z = np.full(m, np.nan, dtype=complex)
+    for lane in range(nbf // 2):
+        z = lane == 0
+        j0 = lane
+        j1 = nbf // 2 if z else nbf - lane
+        a0 = nbf // 2 if z else j0
+        wa = w[a0]
+        wb = 1.0 if z else wa
+        u = [None] * (2 * R)
+        for r in range(R):
+            if r < G:
+                e = a0 + r * nbf
+                tw = wa if r == 0 else wa * w[r * nbf]
+            else:
+                p = r - G + 1
+                e = p * nbf if z else j0 + r * nbf
+                tw = wb * w[(p if z else r) * nbf]
+            u[r], u[2 * R - 1 - r] = pair(xh[e], xh[m - e], tw)
+        v = [u[lane0_slot(k)] if z else u[k] for k in range(2 * R)]
+        if z:
+            x0, xn = xh[0].real + 0j, xh[m].real + 0j
+            v[0] = pair(x0, xn, 1.0)[0]
+        for r in range(R):
+            Z[j0 + r * nbf] = v[r]
+            Z[j1 + r * nbf] = v[R + r]
+    return Z
+
+
+def fused_r2c_last_stage(Z: np.ndarray, R: int, forward: bool) -> np.ndarray:
+    """static_fft.cu FusedR2C::run after the last stage's butterflies: the
+    thread that owns butterflies j0, j1 = NBF - j0 (lane 0: 0, NBF/2) holds
+    Z[j + r NBF] and writes the m+1 bins X[k] = S/2 + w^k U/2,
+    X[m-k] = conj(S/2 - w^k U/2) through the common pair loop (lane 0 with
+    its operands selected).  Returns X (length m + 1)."""
+    m = len(Z)
+    nbf = m // R
+    G = (R + 1) // 2
+    w = np.exp((-1 if forward else 1) * 2j * np.pi * np.arange(m + 1) / (2 * m))
+
+    def pair(zk, zm, tw):
+        s = zk + np.conj(zm)
+        u = -1j * (zk - np.conj(zm))
+        return s / 2 + tw * u / 2, np.conj(s / 2 - tw * u / 2)
+
+    X = np.full(m + 1, np.nan, dtype=complex)
+    for lane in range(nbf // 2):
+        z = lane == 0
+        j0 = lane
+        j1 = nbf // 2 if z else nbf - lane
+        v = [Z[j0 + r * nbf] for r in range(R)] + [Z[j1 + r * nbf] for r in range(R)]
+        u = [None] * (2 * R)
+        for r in range(R):
+            if r < G:
+                u[r] = v[R + r] if z else v[r]
+                u[2 * R - 1 - r] = v[2 * R - 1 - r]
+            else:
+                p = r - G + 1
+                u[r] = v[p] if z else v[r]
+                u[2 * R - 1 - r] = v[R - p] if z else v[2 * R - 1 - r]
+        a0 = nbf // 2 if z else j0
+        wa = w[a0]
+        wb = 1.0 if z else wa
+        for r in range(R):
+            if r < G:
+                o1, o2 = a0 + r * nbf, j1 + (R - 1 - r) * nbf
+                tw = wa if r == 0 else wa * w[r * nbf]
+            else:
+                p = r - G + 1
+                o1 = p * nbf if z else j0 + r * nbf
+                o2 = (R - p) * nbf if z else j1 + (R - 1 - r) * nbf
+                tw = wb * w[(p if z else r) * nbf]
+            X[o1], X[o2] = pair(u[r], u[2 * R - 1 - r], tw)
+        if z:
+            X[0], X[m] = pair(v[0], v[0], 1.0)
+    return X

@@ -51,3 +51,33 @@ def test_reciprocal_modulo_exact():
         m = np.uint64(((1 << 32) + ns - 1) // ns)
         q = (j * m) >> np.uint64(32)
         assert np.array_equal(j - q * np.uint64(ns), j % np.uint64(ns)), ns
+
+
+@pytest.mark.parametrize("n,R", [(4096, 8), (3000, 5), (256, 8), (2048, 8), (4096, 16), (1000, 5)])
+@pytest.mark.parametrize("fwd", [True, False])
+def test_fused_c2r_first_stage(n, R, fwd):
+    """Mirror-owned first stage of a C2R engine: every packed input Z[e] built once, as C2RPre would."""
+    m = n // 2
+    rng = np.random.default_rng(n + R)
+    xh = rng.standard_normal(m + 1) + 1j * rng.standard_normal(m + 1)
+    w = np.exp((-1 if fwd else 1) * 2j * np.pi * np.arange(m) / n)
+    x0, xm = xh.copy(), xh[::-1].copy()
+    x0[0] = x0[0].real
+    xm[0] = xm[0].real  # X[m] seen by e = 0
+    xm[m] = xm[m].real
+    ref = (x0[:m] + np.conj(xm[:m])) + 1j * w * (x0[:m] - np.conj(xm[:m]))
+    z = sm.fused_c2r_first_stage(xh, m, R, fwd)
+    assert not np.isnan(z).any()
+    assert np.allclose(z, ref, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("n,R", [(4096, 8), (3000, 5), (256, 8), (2048, 8), (4096, 16), (1000, 5)])
+@pytest.mark.parametrize("fwd", [True, False])
+def test_fused_r2c_last_stage(n, R, fwd):
+    """Mirror-owned last stage of an R2C engine: all m+1 bins written, equal to the R2C of the real input."""
+    rng = np.random.default_rng(n * R)
+    x = rng.standard_normal(n)
+    Z = np.fft.fft(x[0::2] + 1j * x[1::2]) if fwd else np.fft.ifft(x[0::2] + 1j * x[1::2]) * (n // 2)
+    X = sm.fused_r2c_last_stage(Z, R, fwd)
+    assert not np.isnan(X).any()
+    assert oracle.rel_l2(X, oracle.r2c(x, fwd)) < 1e-12
