@@ -85,4 +85,11 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
+// Output element store that allocates no L1 line: streamed FFT output would
+// otherwise evict the twiddle tables that the next tiles read from L1.
+__device__ __forceinline__ void st_stream(float2 *p, float2 v)
+{
+    asm volatile("st.global.L1::no_allocate.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(v.x), "f"(v.y) : "memory");
+}
+
 }  // namespace sipfft

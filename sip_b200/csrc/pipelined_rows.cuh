@@ -80,7 +80,7 @@ __device__ __forceinline__ void r2c_pair(float2 zk, float2 zm, float2 w, float2 
 
 struct GlobalRow {
     float2 *row;
-    __device__ __forceinline__ void operator()(int e, float2 v) const { row[e] = v; }
+    __device__ __forceinline__ void operator()(int e, float2 v) const { st_stream(row + e, v); }
 };
 
 // R2C post-twiddle from the padded work row to HBM, one pair (k, n-k) per

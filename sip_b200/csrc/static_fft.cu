@@ -272,13 +272,13 @@ struct FusedR2C {
                 w = cmul(wb, __ldg(tw + (z ? p : r) * NBF));
             }
             r2c_pair(u[r], u[2 * R - 1 - r], dir<FWD>(w), a, b);
-            y[o1] = a;
-            y[o2] = b;
+            st_stream(y + o1, a);
+            st_stream(y + o2, b);
         }
         if (z) {
             r2c_pair(v[0], v[0], make_float2(1.f, 0.f), a, b);
-            y[0] = a;
-            y[N] = b;
+            st_stream(y, a);
+            st_stream(y + N, b);
         }
     }
 
@@ -295,8 +295,8 @@ struct FusedR2C {
             for (int r = 0; r < R; r++) {
                 const float2 w = r == 0 ? w0 : cmul(w0, __ldg(tw + r * NBF));
                 r2c_pair(v[r], v[2 * R - 1 - r], dir<FWD>(w), a, b);
-                y[j0 + r * NBF] = a;
-                y[j1 + (R - 1 - r) * NBF] = b;
+                st_stream(y + j0 + r * NBF, a);
+                st_stream(y + j1 + (R - 1 - r) * NBF, b);
             }
         } else {
             // bins r NBF pair with (R-r) NBF (r = 0: with the Nyquist bin N),
@@ -304,8 +304,8 @@ struct FusedR2C {
 #pragma unroll
             for (int r = 0; 2 * r <= R; r++) {
                 r2c_pair(v[r], v[(R - r) % R], dir<FWD>(__ldg(tw + r * NBF)), a, b);
-                y[r * NBF] = a;
-                if (2 * r != R) y[N - r * NBF] = b;
+                st_stream(y + r * NBF, a);
+                if (2 * r != R) st_stream(y + N - r * NBF, b);
             }
             const float2 wh = __ldg(tw + NBF / 2);
 #pragma unroll
@@ -313,8 +313,8 @@ struct FusedR2C {
                 const int k = NBF / 2 + r * NBF;
                 const float2 w = r == 0 ? wh : cmul(wh, __ldg(tw + r * NBF));
                 r2c_pair(v[R + r], v[2 * R - 1 - r], dir<FWD>(w), a, b);
-                y[k] = a;
-                if (2 * r != R - 1) y[N - k] = b;
+                st_stream(y + k, a);
+                if (2 * r != R - 1) st_stream(y + N - k, b);
             }
         }
     }

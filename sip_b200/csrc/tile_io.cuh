@@ -229,7 +229,7 @@ __device__ __forceinline__ void store_tile(const TileDesc &d, void *out, const f
     }
     const int count = (io == IO_R2C_FULL) ? n / 2 + 1 : n;
     float2 *y = static_cast<float2 *>(out) + base;
-    for (int e = e0; e < count; e += estep) y[e * es] = row[pad(e)];
+    for (int e = e0; e < count; e += estep) st_stream(y + e * es, row[pad(e)]);
 }
 
 // ------------------------------------------------------------------------------------ async tile loads
