@@ -106,6 +106,9 @@ struct TileDesc {
     int planar;
     const float *in_im;
     float *out_im;
+    // Shared-memory buffers of a row kernel, each g_ns float2: 2 (double-
+    // buffered tiles; 0 reads as 2) or 3 (plus a ping-pong work area).
+    int row_bufs;
 };
 
 // One segment of an uneven batch: a tile-kernel step whose source and

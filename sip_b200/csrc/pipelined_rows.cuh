@@ -102,24 +102,25 @@ __device__ __forceinline__ void r2c_post_row(const float2 *work, float2 *y, int 
 
 template <int MAXE>
 struct RuntimeEngine {
+    static constexpr bool kPingPong = false;
     static constexpr int kMaxThreads = 512;
     static constexpr int kMinBlocks = 1;
     template <bool FWD, class Src0, class DstL>
     __device__ __forceinline__ static void run(const TileDesc &d, float2 *work, const Src0 &src0, const DstL &dstL,
-                                               bool dst_in_place, int lane, bool active)
+                                               bool dst_in_place, int lane, bool active, float2 * = nullptr)
     {
         run_fft<MAXE, FWD>(d, work, src0, true, dstL, dst_in_place, lane, active);
     }
     template <bool FWD, class DstL>
     __device__ __forceinline__ static void run_c2r(const TileDesc &d, float2 *work, const float2 *x, const DstL &dstL,
-                                                   int lane, bool active)
+                                                   int lane, bool active, float2 * = nullptr)
     {
         run_fft<MAXE, FWD>(d, work, C2RPre<FWD>{x, d.n, d.tw}, true, dstL, false, lane, active);
     }
     // R2C: packed FFT into the work row, then the post-twiddle pass to HBM
     template <bool FWD, class Src0>
     __device__ __forceinline__ static void run_r2c(const TileDesc &d, float2 *work, const Src0 &src0, float2 *y,
-                                                   int lane, bool active)
+                                                   int lane, bool active, float2 * = nullptr)
     {
         run_fft<MAXE, FWD>(d, work, src0, true, SmemRow{work}, true, lane, active);
         __syncthreads();
@@ -193,16 +194,17 @@ __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
         }
         const bool active = thread_on && l < rows;
         float2 *work = buf + l * d.pitch;
+        float2 *work2 = Engine::kPingPong ? bufs + 2 * buf_f2 + l * d.pitch : nullptr;
         const int64_t row_index = t * tb + l;
         if constexpr (IO == IO_C2C) {
             Engine::template run<FWD>(d, work, StageRow{stage + l * in_dist},
-                                      GlobalRow{out + row_index * out_dist}, false, lane, active);
+                                      GlobalRow{out + row_index * out_dist}, false, lane, active, work2);
         } else if constexpr (IO == IO_C2R_PACKED) {
             Engine::template run_c2r<FWD>(d, work, stage + l * in_dist, GlobalRow{out + row_index * out_dist}, lane,
-                                          active);
+                                          active, work2);
         } else {  // IO_R2C_PACKED
             Engine::template run_r2c<FWD>(d, work, StageRow{stage + l * in_dist}, out + row_index * out_dist, lane,
-                                          active);
+                                          active, work2);
         }
         __syncthreads();  // buffer b is free for the copy issued in iteration i+1
     }

@@ -424,6 +424,7 @@ struct Builder {
             d.out_a = Addr{out_dist, 0, 1, 0, 0};
             d.g_ns = buf;
             d.tpt = c.tpt;
+            if (sk) d.row_bufs = sk->row_bufs;
             if (row_kernel_smem(d) > static_cast<size_t>(kMaxSmemBytes)) continue;
             const void *fn = nullptr;
             if (sk) {

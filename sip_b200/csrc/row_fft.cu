@@ -34,7 +34,10 @@ const void *pick(const TileDesc &d, int maxe, bool forward)
 
 }  // namespace
 
-size_t row_kernel_smem(const TileDesc &d) { return 128 + 2 * static_cast<size_t>(d.g_ns) * sizeof(float2); }
+size_t row_kernel_smem(const TileDesc &d)
+{
+    return 128 + (d.row_bufs > 2 ? d.row_bufs : 2) * static_cast<size_t>(d.g_ns) * sizeof(float2);
+}
 
 // Raises a kernel's dynamic shared-memory limit to what the SM allows next
 // to the kernel's static shared memory.

@@ -62,6 +62,7 @@ struct StaticKernel {
     int tpt = 0;
     const void *fn[2][3] = {};  // [forward][C2C, R2C packed, C2R packed]
     const void *db[2] = {};     // [forward] double-buffered C2C tiles (strided axes, multi-pass steps)
+    int row_bufs = 2;           // shared-memory buffers of its row kernel (3: ping-pong work area)
 };
 const StaticKernel *find_static_kernel(int n, int io);
 cudaError_t fill_stage_twiddles(float2 *t, const int *radix, int nstages, cudaStream_t st);

@@ -168,24 +168,37 @@ __device__ __forceinline__ void sscatter(const float2 *v, const Dst &dst, int la
     }
 }
 
+// Work row of boundary b (the layout stage b writes and stage b+1 reads).
+// With a ping-pong area (PP) even boundaries live in work2 and odd ones in
+// work, so that no stage scatters over the row it gathers from and the
+// barrier between a stage's gather and its scatter goes away.
+template <bool PP, int B>
+__device__ __forceinline__ float2 *bbuf(float2 *work, float2 *work2)
+{
+    return (PP && B % 2 == 0) ? work2 : work;
+}
+
 // Stage S of the static FFT; stage 0 reads src0 (the staging rows, which
 // alias the work buffer), the last stage writes dstL.
-template <class Q, int T, class PD, bool FWD, int S, class Src0, class DstL>
-__device__ __forceinline__ void srun(float2 *v, float2 *work, const Src0 &src0, const DstL &dstL, bool dst_in_place,
-                                     int lane, bool active, const float2 *stw)
+template <class Q, int T, class PD, bool PP, bool FWD, int S, class Src0, class DstL>
+__device__ __forceinline__ void srun(float2 *v, float2 *work, float2 *work2, const Src0 &src0, const DstL &dstL,
+                                     bool dst_in_place, int lane, bool active, const float2 *stw)
 {
     constexpr bool last = S == Q::S - 1;
     if constexpr (S == 0)
         sgather<Q, 0, T, FWD>(v, src0, lane, active, stw);
     else
-        sgather<Q, S, T, FWD>(v, BoundaryRow<PD, S - 1>{work}, lane, active, stw);
-    if (!last || dst_in_place) __syncthreads();
+        sgather<Q, S, T, FWD>(v, BoundaryRow<PD, S - 1>{bbuf<PP, S - 1>(work, work2)}, lane, active, stw);
     if constexpr (last) {
+        // an in-place destination is the work row: wait while it is still gathered from
+        constexpr bool src_is_work = S == 0 || !(PP && (S - 1) % 2 == 0);
+        if (dst_in_place && src_is_work) __syncthreads();
         sscatter<Q, S, T>(v, dstL, lane, active);
     } else {
-        sscatter<Q, S, T>(v, BoundaryRow<PD, S>{work}, lane, active);
+        if constexpr (!PP) __syncthreads();
+        sscatter<Q, S, T>(v, BoundaryRow<PD, S>{bbuf<PP, S>(work, work2)}, lane, active);
         __syncthreads();
-        srun<Q, T, PD, FWD, S + 1>(v, work, src0, dstL, dst_in_place, lane, active, stw);
+        srun<Q, T, PD, PP, FWD, S + 1>(v, work, work2, src0, dstL, dst_in_place, lane, active, stw);
     }
 }
 
@@ -383,32 +396,33 @@ struct FusedC2R {
     }
 };
 
-template <class Q, int T, class PD = Pads<>>
+template <class Q, int T, class PD = Pads<>, bool PP = false>
 struct StaticEngine {
+    static constexpr bool kPingPong = PP;  // a third shared-memory buffer holds the even boundaries
     static constexpr int kMaxThreads = T <= 256 ? 256 : T;
     // 3 CTAs per SM (<= 80 registers) unless a thread holds more than 16 points
     static constexpr int kMinBlocks = T <= 256 ? (Q::N / T > 16 ? 2 : 3) : 1;
     template <bool FWD, class Src0, class DstL>
     __device__ __forceinline__ static void run(const TileDesc &d, float2 *work, const Src0 &src0, const DstL &dstL,
-                                               bool dst_in_place, int lane, bool active)
+                                               bool dst_in_place, int lane, bool active, float2 *work2 = nullptr)
     {
         float2 v[static_maxv<Q, T>()];
-        srun<Q, T, PD, FWD, 0>(v, work, src0, dstL, dst_in_place, lane, active, d.stw);
+        srun<Q, T, PD, PP, FWD, 0>(v, work, work2, src0, dstL, dst_in_place, lane, active, d.stw);
     }
 
     template <bool FWD, class Src0>
     __device__ __forceinline__ static void run_r2c(const TileDesc &d, float2 *work, const Src0 &src0, float2 *y,
-                                                   int lane, bool active)
+                                                   int lane, bool active, float2 *work2 = nullptr)
     {
         using F = FusedR2C<Q, T, PD, FWD>;
         if constexpr (F::ok) {
             constexpr int V = static_maxv<Q, T>() > 2 * F::R ? static_maxv<Q, T>() : 2 * F::R;
             float2 v[V];
-            srun_prefix<FWD>(v, work, src0, lane, active, d.stw);
+            prefix<FWD, 0>(v, work, work2, src0, lane, active, d.stw);
             __syncthreads();
-            F::run(v, work, y, lane, active, d.stw, d.tw);
+            F::run(v, bbuf<PP, Q::S - 2>(work, work2), y, lane, active, d.stw, d.tw);
         } else {
-            run<FWD>(d, work, src0, SmemRow{work}, true, lane, active);
+            run<FWD>(d, work, src0, SmemRow{work}, true, lane, active, work2);
             __syncthreads();
             if (active) r2c_post_row<FWD>(work, y, d.n, lane, d.tpt, d.tw);
         }
@@ -418,7 +432,7 @@ struct StaticEngine {
     // the packed inputs pairwise, else every element goes through C2RPre.
     template <bool FWD, class DstL>
     __device__ __forceinline__ static void run_c2r(const TileDesc &d, float2 *work, const float2 *x, const DstL &dstL,
-                                                   int lane, bool active)
+                                                   int lane, bool active, float2 *work2 = nullptr)
     {
         using F = FusedC2R<Q, T, FWD>;
         if constexpr (F::ok) {
@@ -431,9 +445,9 @@ struct StaticEngine {
                 dft<R, FWD>(v);
                 dft<R, FWD>(v + R);
             }
-            __syncthreads();  // the staged spectrum is read in full before the work layout overwrites it
+            if constexpr (!PP) __syncthreads();  // the staged spectrum is read before the work row overwrites it
             if (active) {
-                const BoundaryRow<PD, 0> w{work};
+                const BoundaryRow<PD, 0> w{bbuf<PP, 0>(work, work2)};
 #pragma unroll
                 for (int r = 0; r < R; r++) {
                     w(j0 * R + r, v[r]);
@@ -441,32 +455,26 @@ struct StaticEngine {
                 }
             }
             __syncthreads();
-            srun<Q, T, PD, FWD, 1>(v, work, SmemRow{work}, dstL, false, lane, active, d.stw);
+            srun<Q, T, PD, PP, FWD, 1>(v, work, work2, SmemRow{work}, dstL, false, lane, active, d.stw);
         } else {
-            run<FWD>(d, work, C2RPre<FWD>{x, d.n, d.tw}, dstL, false, lane, active);
+            run<FWD>(d, work, C2RPre<FWD>{x, d.n, d.tw}, dstL, false, lane, active, work2);
         }
     }
 
-    // every stage but the last, leaving the data in the padded work row
-    template <bool FWD, class Src0>
-    __device__ __forceinline__ static void srun_prefix(float2 *v, float2 *work, const Src0 &src0, int lane,
-                                                       bool active, const float2 *stw)
-    {
-        prefix<FWD, 0>(v, work, src0, lane, active, stw);
-    }
+    // every stage but the last, leaving the data in the work row of boundary S-2
     template <bool FWD, int S, class Src0>
-    __device__ __forceinline__ static void prefix(float2 *v, float2 *work, const Src0 &src0, int lane, bool active,
-                                                  const float2 *stw)
+    __device__ __forceinline__ static void prefix(float2 *v, float2 *work, float2 *work2, const Src0 &src0, int lane,
+                                                  bool active, const float2 *stw)
     {
         if constexpr (S < Q::S - 1) {
             if constexpr (S == 0)
                 sgather<Q, 0, T, FWD>(v, src0, lane, active, stw);
             else
-                sgather<Q, S, T, FWD>(v, BoundaryRow<PD, S - 1>{work}, lane, active, stw);
-            __syncthreads();
-            sscatter<Q, S, T>(v, BoundaryRow<PD, S>{work}, lane, active);
+                sgather<Q, S, T, FWD>(v, BoundaryRow<PD, S - 1>{bbuf<PP, S - 1>(work, work2)}, lane, active, stw);
+            if constexpr (!PP) __syncthreads();
+            sscatter<Q, S, T>(v, BoundaryRow<PD, S>{bbuf<PP, S>(work, work2)}, lane, active);
             if constexpr (S + 1 < Q::S - 1) __syncthreads();
-            prefix<FWD, S + 1>(v, work, src0, lane, active, stw);
+            prefix<FWD, S + 1>(v, work, work2, src0, lane, active, stw);
         }
     }
 };
@@ -540,7 +548,7 @@ constexpr bool pads_fit()
     return true;
 }
 
-template <class Q, int T, class PD = Pads<>>
+template <class Q, int T, class PD = Pads<>, bool PP = false>
 StaticKernel make_entry(int io_mask = 7)
 {
     static_assert(pads_fit<Q, PD>(), "padded work row exceeds the planner's pitch");
@@ -550,15 +558,18 @@ StaticKernel make_entry(int io_mask = 7)
     e.nstages = Q::S;
     for (int s = 0; s < Q::S; s++) e.radix[s] = Q::r[s];
     e.tpt = T;
-    using E = StaticEngine<Q, T, PD>;
+    using E = StaticEngine<Q, T, PD, PP>;
+    e.row_bufs = PP ? 3 : 2;
     e.fn[1][0] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, true, IO_C2C>);
     e.fn[1][1] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, true, IO_R2C_PACKED>);
     e.fn[1][2] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, true, IO_C2R_PACKED>);
     e.fn[0][0] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, false, IO_C2C>);
     e.fn[0][1] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, false, IO_R2C_PACKED>);
     e.fn[0][2] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, false, IO_C2R_PACKED>);
-    e.db[1] = reinterpret_cast<const void *>(static_db_kernel<E, true>);
-    e.db[0] = reinterpret_cast<const void *>(static_db_kernel<E, false>);
+    if constexpr (!PP) {  // the double-buffered tile kernel has no ping-pong area
+        e.db[1] = reinterpret_cast<const void *>(static_db_kernel<E, true>);
+        e.db[0] = reinterpret_cast<const void *>(static_db_kernel<E, false>);
+    }
     return e;
 }
 
@@ -579,8 +590,9 @@ const std::vector<StaticKernel> &registry()
         // post-twiddle fuses into it; C2C and C2R on 10 x 10 x 15, one
         // butterfly per thread in the radix-10 stages; both with per-boundary
         // work-row layouts that halve the bank-conflicting shared-memory words
-        make_entry<Seq<12, 5, 5, 5>, 150, Pads<1, 48, 1, 0, 1, 0>>(4),
-        make_entry<Seq<10, 10, 15>, 150, Pads<1, 80, 3, 50>>(3),
+        make_entry<Seq<12, 5, 5, 5>, 150, Pads<1, 48, 1, 0, 1, 0>, true>(4),
+        make_entry<Seq<10, 10, 15>, 150, Pads<1, 80, 3, 50>, true>(2),
+        make_entry<Seq<10, 10, 15>, 150, Pads<1, 80, 3, 50>>(1),
     };
     return r;
 }
@@ -592,7 +604,7 @@ void static_kernel_fns(std::vector<const void *> &out)
     for (const StaticKernel &e : registry())
         for (int f = 0; f < 2; f++) {
             for (int io = 0; io < 3; io++) out.push_back(e.fn[f][io]);
-            out.push_back(e.db[f]);
+            if (e.db[f]) out.push_back(e.db[f]);
         }
 }
 
