@@ -581,7 +581,10 @@ const std::vector<StaticKernel> &registry()
         make_entry<Seq<16, 16>, 16>(),          // 256
         make_entry<Seq<16, 16, 2>, 32>(),       // 512
         make_entry<Seq<16, 16, 4>, 64>(),       // 1024
-        make_entry<Seq<8, 16, 16>, 128>(2),     // 2048, C2R: pre-twiddle fused into the radix-8 first stage
+        // 2048, C2R: pre-twiddle fused into the radix-8 first stage, ping-pong
+        // work rows (4 CTAs per SM instead of 6, measured 3 % faster; the R2C
+        // engine measured the same either way and keeps 6)
+        make_entry<Seq<8, 16, 16>, 128, Pads<>, true>(2),
         make_entry<Seq<16, 16, 8>, 128, Pads<1, 16, 1, 128>>(),  // 2048
         make_entry<Seq<16, 16, 16>, 256>(),     // 4096
         make_entry<Seq<16, 16, 16, 2>, 512>(),  // 8192
