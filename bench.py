@@ -220,6 +220,82 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------------- multi-axis configs
+MULTIAXIS = (("2d_2048x2048_b8", [2048, 2048], 8), ("3d_256x256x256_b1", [256, 256, 256], 1))
+FORM_NAMES = ("fp32", "fp16x3", "bf16x3")
+
+
+def multiaxis_measure(sizes, batch: int, form: str, reps: int, flush_l2) -> dict:
+    """One C2C plan (FORWARD) over device-resident data: median CUDA-event time of
+    `reps` executions with the L2 flushed before each, GFLOP/s, algorithmic-byte
+    roofline, and the error of the first transform of the batch against FP64."""
+    import torch
+
+    from sip_b200 import fft
+
+    prec = {"fp32": fft.PRECISION_FP32, "fp16x3": fft.PRECISION_FP16X3, "bf16x3": fft.PRECISION_BF16X3}[form]
+    g = torch.Generator(device="cuda").manual_seed(31)
+    shape = [batch] + list(sizes)
+    x = torch.complex(torch.rand(shape, device="cuda", generator=g) * 2 - 1,
+                      torch.rand(shape, device="cuda", generator=g) * 2 - 1)
+    y = torch.empty_like(x)
+    plan = fft.FftPlan(sizes, fft.ASCEND_FFT_C2C, fft.ASCEND_FFT_FORWARD, batch, precision=prec)
+    plan(x, y)
+    for _ in range(2):
+        plan.exec_raw(x.data_ptr(), y.data_ptr())
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        flush_l2(plan.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(plan.stream)
+        plan.exec_raw(x.data_ptr(), y.data_ptr())
+        e1.record(plan.stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    from oracle import oracle as _oracle  # checker only
+
+    xs = x[:1].cpu().numpy()
+    ref = _oracle.c2c(xs, True, ndim=len(sizes))
+    ys = y[:1].cpu().numpy()
+    n_total = int(np.prod(sizes))
+    med = statistics.median(ms)
+    peak, _ = measured_peak_hbm()
+    nbytes = 16 * n_total * batch
+    out = {"ms": med, "GFLOPps": 5.0 * n_total * math.log2(n_total) * batch / (med / 1e3) / 1e9,
+           "GBps": nbytes / (med / 1e3) / 1e9, "frac_of_hbm": nbytes / (med / 1e3) / 1e9 / peak,
+           "rel_l2": _oracle.rel_l2(ys, ref), "max_abs": _oracle.max_abs(ys, ref),
+           "bound": _oracle.tolerance(n_total), "launches": plan.launches(),
+           "tensor_core": "tensor-core" in plan.describe()}
+    plan.close()
+    return out
+
+
+def config_extras(args, flush_l2) -> dict:
+    """The other workload configurations, a few seconds each, for the bench line:
+    C3 multi-axis transforms per arithmetic form (with the tensor-core / plain
+    ratio), C4 uneven batch, C5 serving at four offered loads per form."""
+    ex = {}
+    c3 = {}
+    for name, sizes, batch in MULTIAXIS:
+        per = {}
+        for form in FORM_NAMES:
+            per[form] = multiaxis_measure(sizes, batch, form, args.extra_reps, flush_l2)
+        for form in FORM_NAMES[1:]:
+            per[f"{form}_over_fp32"] = per["fp32"]["ms"] / per[form]["ms"]
+        c3[name] = per
+    ex["c3_multiaxis"] = {"workload": "C2C complex64 FORWARD, uniform[-1,1] inputs; L2 flushed before each of "
+                                      f"{args.extra_reps} timed executions; error of the first transform vs FP64",
+                          "results": c3}
+    ex["c4_uneven"] = dict(uneven_measure(20000, max(3, args.extra_reps // 2), 3), workload="20000 " + UNEVEN_WORKLOAD)
+    c5 = {}
+    for form in ("fp32", "fp16x3"):
+        c5[form] = serving_points(form, True, [1000.0, 5000.0, 20000.0, 50000.0], 0.25, 2000, 4)
+    ex["c5_serving"] = {"workload": SERVE_WORKLOAD + "; device-resident request buffers; 4 lanes",
+                        "points": c5}
+    return ex
+
+
 # ----------------------------------------------------------------------------------- our arm
 def run_ours(args, world, rank, local):
     import ctypes
@@ -278,17 +354,18 @@ def run_ours(args, world, rank, local):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     flush_read = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
-    def flush_l2(sync=True):
+    def flush_l2(sync=True, on=None):
         # write a buffer larger than L2, then read another one: the dirty lines
         # of the write are written back here, outside the timed region.  The
         # flush runs on the benchmark stream, so a step's first event is recorded
         # after it completes; without the synchronize the host enqueues the step
         # while the flush still runs, and no launch gap enters the timed region.
-        with torch.cuda.stream(stream):
+        st = on if on is not None else stream
+        with torch.cuda.stream(st):
             flush.fill_(1.0)
             flush_read.sum()
         if sync:
-            stream.synchronize()
+            st.synchronize()
 
     # ---------------- accuracy of the round trip on this data
     with torch.cuda.stream(stream):
@@ -317,7 +394,7 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     nlaunch = 2 * len(SIZES)
     step_ms, launch_ms = [], [[] for _ in range(nlaunch)]
-    sampler = ClockSampler(local) if rank == 0 or True else None
+    sampler = ClockSampler(local)  # every rank samples its own GPU
     sampler.start()
     time.sleep(0.3)
     for _ in range(args.steps):
@@ -408,6 +485,9 @@ def run_ours(args, world, rank, local):
     e2e_value = step_flops() * args.steps * world / e2e_s / 1e9
 
     launches_per_step = sum(f.launches() + g.launches() for _, f, g in plans)
+    extras = None
+    if world == 1 and not args.no_extras:
+        extras = config_extras(args, lambda st: flush_l2(sync=False, on=st))
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -432,6 +512,8 @@ def run_ours(args, world, rank, local):
             "clocks": clocks,
             "accuracy": acc,
         }
+        if extras is not None:
+            line.update(extras)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
@@ -449,17 +531,21 @@ def run_ours(args, world, rank, local):
 
 
 # ----------------------------------------------------------------------------------- uneven batch
-def run_uneven(args, world, rank, local):
-    """20 000 1D C2C transforms of uneven lengths in one persistent, graph-captured launch."""
+UNEVEN_WORKLOAD = ("1D C2C complex64 transforms, lengths log-uniform in [64, 65536] snapped to 7-smooth, "
+                   "Zipf(1.2) batch per length capped at 512; one persistent launch replayed from a CUDA graph")
+
+
+def uneven_measure(total: int, steps: int, warmup: int, autotune: bool = False) -> dict:
+    """The uneven batch in one persistent, graph-captured launch: per-step time
+    (CUDA events on the launching stream), GFLOP/s and algorithmic-byte roofline."""
     import torch
 
     from sip_b200 import fft, workloads
 
-    torch.cuda.set_device(local)
-    groups = workloads.uneven_batch_set(total=args.uneven_total, seed=2024)
+    groups = workloads.uneven_batch_set(total=total, seed=2024)
     fl, alg_bytes = workloads.uneven_flops_bytes(groups)
     cache = os.path.join(ROOT, "sip_b200", "tune", "b200_c2c_fp32.jsonl")
-    if args.autotune:
+    if autotune:
         os.makedirs(os.path.dirname(cache), exist_ok=True)
         fft.autotune(groups, fft.ASCEND_FFT_FORWARD, cache)
     plan = fft.BatchPlan(groups, fft.ASCEND_FFT_FORWARD, cache if os.path.exists(cache) else None)
@@ -467,48 +553,61 @@ def run_uneven(args, world, rank, local):
     y = torch.empty_like(x)
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
-        for _ in range(max(3, args.warmup)):
+        for _ in range(max(3, warmup)):
             plan(x, y, stream=stream)
     stream.synchronize()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     ms = []
-    for _ in range(args.steps):
+    for _ in range(steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         with torch.cuda.stream(stream):
             ev[0].record(stream)
             plan(x, y, stream=stream)
             ev[1].record(stream)
         stream.synchronize()
         ms.append(ev[0].elapsed_time(ev[1]))
-    t = max_over_ranks(sum(ms) / 1e3, world)
+    plan.close()
     peak, kind = measured_peak_hbm()
-    achieved = alg_bytes / (t / args.steps) / 1e9
+    t = sum(ms) / 1e3 / steps
+    return {"ms_per_step": t * 1e3, "GFLOPps": fl / t / 1e9, "groups": len(groups), "transforms": total,
+            "bytes_in": alg_bytes // 2, "tuned": os.path.exists(cache),
+            "roofline": {"bound": "hbm", "achieved": alg_bytes / t / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg_bytes / t / 1e9 / peak, "peak_source": kind,
+                         "algorithmic_bytes_per_step": alg_bytes},
+            "launches_per_step": 1, "l2": f"inputs ({alg_bytes // 2 / 1e9:.2f} GB) larger than L2"}
+
+
+def run_uneven(args, world, rank, local):
+    """20 000 1D C2C transforms of uneven lengths in one persistent, graph-captured launch."""
+    import torch
+
+    torch.cuda.set_device(local)
+    r = uneven_measure(args.uneven_total, args.steps, args.warmup, args.autotune)
+    t = max_over_ranks(r["ms_per_step"] / 1e3 * args.steps, world)
     if rank == 0:
         print(json.dumps({
-            "metric": "FFT GFLOP/s (5N*log2N per transform), uneven batch", "value": fl * args.steps * world / t / 1e9,
+            "metric": "FFT GFLOP/s (5N*log2N per transform), uneven batch", "value": r["GFLOPps"] * world,
             "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "dtype": "f32",
             "data": "synthetic (seeded lengths/batches, randn values)",
-            "config": {"workload": f"{args.uneven_total} 1D C2C complex64 transforms, lengths log-uniform in [64, 65536] snapped to "
-                                   "7-smooth, Zipf(1.2) batch per length capped at 512; one persistent launch "
-                                   "replayed from a CUDA graph", "groups": len(groups), "transforms": args.uneven_total,
-                       "bytes_in": alg_bytes // 2, "tuned": os.path.exists(cache)},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": kind, "algorithmic_bytes_per_step": alg_bytes},
-            "gpu_launches": args.steps,
+            "config": {"workload": f"{args.uneven_total} {UNEVEN_WORKLOAD}", "groups": r["groups"],
+                       "transforms": args.uneven_total, "bytes_in": r["bytes_in"], "tuned": r["tuned"]},
+            "roofline": r["roofline"], "gpu_launches": args.steps,
         }), flush=True)
-    plan.close()
 
 
 # ----------------------------------------------------------------------------------- serving
-def run_serving(args, world, rank, local):
-    """Poisson arrivals over a swept offered load into the C++ continuous-batching server."""
+SERVE_SIZES = (4096, 8192, 16384, 65536)
+
+
+def serving_points(precision_name: str, device_io: bool, rates, seconds: float, max_requests: int,
+                   lanes: int) -> list[dict]:
+    """Poisson arrivals into the C++ continuous-batching server at each offered
+    load; p50/p99 latency, achieved request rate and throughput per load."""
     import torch
 
     from sip_b200 import fft, workloads
 
-    torch.cuda.set_device(local)
-    sizes = (4096, 8192, 16384, 65536)
-    classes = [(t, n) for n in sizes for t in (fft.ASCEND_FFT_C2C, fft.ASCEND_FFT_R2C)]
+    classes = [(t, n) for n in SERVE_SIZES for t in (fft.ASCEND_FFT_C2C, fft.ASCEND_FFT_R2C)]
     rows_min, rows_max = 64, 1024
     rng = np.random.default_rng(5)
     pin, pout, keep = [], [], []
@@ -518,7 +617,7 @@ def run_serving(args, world, rank, local):
             x = np.ascontiguousarray(x.real.astype(np.float32))
         xt = torch.from_numpy(x)
         ot = torch.empty((rows_max, n if t == fft.ASCEND_FFT_C2C else n // 2 + 1), dtype=torch.complex64)
-        if args.device_io:
+        if device_io:
             xt, ot = xt.cuda(), ot.cuda()
         else:
             xt, ot = xt.pin_memory(), ot.pin_memory()
@@ -526,16 +625,16 @@ def run_serving(args, world, rank, local):
         pin.append(xt.data_ptr())
         pout.append(ot.data_ptr())
     precision = {"fp32": fft.PRECISION_FP32, "fp16x3": fft.PRECISION_FP16X3,
-                 "bf16x3": fft.PRECISION_BF16X3}[args.precision]
-    srv = fft.Server(budget_bytes=32 << 30, lanes=args.lanes, max_rows=rows_max, device_io=args.device_io,
+                 "bf16x3": fft.PRECISION_BF16X3}[precision_name]
+    srv = fft.Server(budget_bytes=32 << 30, lanes=lanes, max_rows=rows_max, device_io=device_io,
                      precision=precision)
     for t, n in classes:
         srv.warm(t, fft.ASCEND_FFT_FORWARD, n)
     # warm-up traffic: allocates each lane's staging buffers
-    srv.run_poisson(1e6, 4 * args.lanes * len(classes), 1, classes, pin, pout, rows_max, rows_max)
+    srv.run_poisson(1e6, 4 * lanes * len(classes), 1, classes, pin, pout, rows_max, rows_max)
     points = []
-    for rate in [float(r) for r in args.rates.split(",")]:
-        count = int(min(args.max_requests, max(10, rate * args.seconds)))
+    for rate in rates:
+        count = int(min(max_requests, max(10, rate * seconds)))
         b0 = srv.batches()
         wall, lat, rows, cls = srv.run_poisson(rate, count, 11, classes, pin, pout, rows_min, rows_max)
         ok = lat[lat > 0]
@@ -550,15 +649,27 @@ def run_serving(args, world, rank, local):
                        "achieved_rps": count / wall, "GBps": by / wall / 1e9, "GFLOPps": fl / wall / 1e9,
                        "batches": srv.batches() - b0})
     srv.close()
+    return points
+
+
+SERVE_WORKLOAD = ("Poisson arrivals; R2C or C2C FP32, N in {4096, 8192, 16384, 65536}, rows uniform in "
+                  "[64, 1024], chirp + noise at SNR U[0,20] dB; 32 GiB admission budget")
+
+
+def run_serving(args, world, rank, local):
+    """Poisson arrivals over a swept offered load into the C++ continuous-batching server."""
+    import torch
+
+    torch.cuda.set_device(local)
+    points = serving_points(args.precision, args.device_io, [float(r) for r in args.rates.split(",")],
+                            args.seconds, args.max_requests, args.lanes)
     if rank == 0:
         print(json.dumps({
             "metric": "serving p50/p99 latency (ms) and throughput vs offered load", "unit": "ms",
             "form": {"fp32": "plain FP32", "fp16x3": "split FP16 hi/lo x3 (tensor-core stages where available)",
                      "bf16x3": "split BF16 hi/lo x3 (tensor-core stages where available)"}[args.precision],
             "io": "device-resident buffers" if args.device_io else "pinned host buffers",
-            "config": {"workload": "Poisson arrivals; R2C or C2C FP32, N in {4096, 8192, 16384, 65536}, rows "
-                                   "uniform in [64, 1024], chirp + noise at SNR U[0,20] dB; 32 GiB admission budget",
-                       "lanes": args.lanes, "max_rows": rows_max},
+            "config": {"workload": SERVE_WORKLOAD, "lanes": args.lanes, "max_rows": 1024},
             "points": points}), flush=True)
 
 
@@ -643,6 +754,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline only: skip the C3 multi-axis, C4 uneven and C5 serving keys of the bench line")
+    ap.add_argument("--extra-reps", type=int, default=10, help="timed executions per C3 form")
     ap.add_argument("--e2e-chunk", type=int, default=E2E_CHUNK, help="rows per chunk of the streamed end-to-end step")
     ap.add_argument("--workload", default="roundtrip", choices=["roundtrip", "uneven", "serving", "kernel"])
     ap.add_argument("--kind", default="c2c", choices=["c2c", "r2c", "c2r"], help="(kernel) transform type")

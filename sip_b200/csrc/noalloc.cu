@@ -1,9 +1,9 @@
 // C2C FFT entry point that allocates nothing.
 //
 // Some callers cannot allocate device memory at the moment they need an FFT:
-// real-time loops that forbid allocator calls once they are running, code
-// that runs while its stream is being recorded into a graph, or hosts that
-// hand the library raw buffers and own every allocation themselves.  The
+// real-time loops that forbid allocator calls once they are running, or
+// hosts that hand the library raw buffers and own every allocation
+// themselves.  The
 // ordinary exec path for long transforms needs a caller-provided workspace
 // and a plan whose twiddle tables are allocated with cudaMalloc.  This entry
 // point instead keeps its scratch (the twiddle tables and the intermediate
@@ -189,7 +189,7 @@ extern "C" int32_t asdFftExecC2CNoAlloc(const void *input, void *output, int64_t
         set_last_error("asdFftExecC2CNoAlloc: invalid direction");
         return AsdSip::ACL_ERROR_INVALID_PARAM;
     }
-    if (fftSize * batchSize > kNoAllocDataElems) {
+    if (batchSize > kNoAllocDataElems / fftSize) {  // fftSize * batchSize > kNoAllocDataElems, without overflow
         set_last_error("asdFftExecC2CNoAlloc: fftSize * batchSize exceeds the 1048576-element scratch array");
         return AsdSip::ACL_ERROR_INVALID_PARAM;
     }

@@ -180,10 +180,12 @@ __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
         const int b = i & 1;
         const int64_t tn = t + gridDim.x;
         if (tn < d.num_tiles) issue(tn, b ^ 1);
-        if (!mbar_wait_bounded(&bars[b], (i >> 1) & 1)) {
-            if (tid == 0) atomicExch(err, 1);
-            return;
-        }
+        // A thread whose bounded wait gave up records it and still runs the
+        // tile (on whatever the buffer holds: every access stays in bounds), so
+        // that every thread reaches the same barriers; the CTA leaves together
+        // at the end of the iteration.
+        const bool timed_out = !mbar_wait_bounded(&bars[b], (i >> 1) & 1);
+        if (timed_out) atomicExch(err, 1);
         const int rows = tile_rows(t);
         float2 *buf = bufs + b * buf_f2;
         const int64_t s = t * tb * in_dist, e = min(s + rows * in_dist, total);
@@ -206,7 +208,8 @@ __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
             Engine::template run_r2c<FWD>(d, work, StageRow{stage + l * in_dist}, out + row_index * out_dist, lane,
                                           active, work2);
         }
-        __syncthreads();  // buffer b is free for the copy issued in iteration i+1
+        // buffer b is free for the copy issued in iteration i+1; a CTA-uniform exit after a timeout
+        if (__syncthreads_or(timed_out)) return;
     }
 }
 

@@ -37,6 +37,32 @@ def test_oracle_matches_reference_golden(golden, name, kind, n, fwd):
     assert oracle.rel_l2(y, ref) < 2e-6 * max(1.0, np.log2(max(n, 2))), name
 
 
+GOLDEN_ND = os.path.join(os.path.dirname(__file__), "golden", "reference_vectors_nd.npz")
+
+
+def _nd_cases():
+    z = np.load(GOLDEN_ND)
+    for name, kind, shape, nd, fwd in zip(z["_names"], z["_kinds"], z["_shapes"], z["_ndim"], z["_forward"]):
+        yield str(name), str(kind), tuple(int(v) for v in shape[:nd]), bool(fwd)
+
+
+@pytest.mark.parametrize("name,kind,shape,fwd", list(_nd_cases()))
+def test_oracle_matches_reference_golden_nd(name, kind, shape, fwd):
+    """2D / 3D: the oracle's axis order (R2C on the last axis, C2R last) and
+    per-axis signs against the reference's matrices applied in its plans' order."""
+    z = np.load(GOLDEN_ND)
+    x, ref = z[name + "__in"], z[name + "__out"]
+    nd = len(shape)
+    if kind == "c2c":
+        y = oracle.c2c(x, fwd, ndim=nd)
+    elif kind == "r2c":
+        y = oracle.r2c(x, fwd, ndim=nd)
+    else:
+        y = oracle.c2r(x, shape[-1], fwd, ndim=nd)
+    assert y.shape == ref.shape
+    assert oracle.rel_l2(y, ref) < 2e-6 * max(1.0, np.log2(int(np.prod(shape)))), name
+
+
 @pytest.mark.parametrize("n", [1, 2, 3, 5, 6, 8, 15, 16, 30, 49, 64, 97, 128, 210, 256])
 @pytest.mark.parametrize("fwd", [True, False])
 def test_oracle_vs_direct_dft(n, fwd):
