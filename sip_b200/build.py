@@ -14,6 +14,7 @@ import argparse
 import concurrent.futures as cf
 import glob
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -31,16 +32,31 @@ COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibilit
 CU_FLAGS = ARCH + ["-lineinfo", "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 
 
-def _headers() -> list[str]:
-    return glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
-        glob.glob(os.path.join(ROOT, "include", "*.h"))
+_INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
 
 
-def _stale(obj: str, src: str, newest_header: float) -> bool:
+def _deps(src: str, seen: set[str] | None = None) -> set[str]:
+    """The file and every project header it includes, transitively."""
+    seen = set() if seen is None else seen
+    if src in seen or not os.path.exists(src):
+        return seen
+    seen.add(src)
+    with open(src, encoding="utf-8", errors="replace") as f:
+        text = f.read()
+    for inc in _INCLUDE.findall(text):
+        for base in (os.path.dirname(src), CSRC, os.path.join(ROOT, "include")):
+            path = os.path.normpath(os.path.join(base, inc))
+            if os.path.exists(path):
+                _deps(path, seen)
+                break
+    return seen
+
+
+def _stale(obj: str, src: str) -> bool:
     if not os.path.exists(obj):
         return True
     t = os.path.getmtime(obj)
-    return t < os.path.getmtime(src) or t < newest_header
+    return any(t < os.path.getmtime(d) for d in _deps(src))
 
 
 def _compile(src: str, obj: str, verbose: bool) -> tuple[str, str]:
@@ -64,13 +80,14 @@ def build(clean: bool = False, verbose: bool = False, jobs: int | None = None) -
         shutil.rmtree(BUILD)
     os.makedirs(BUILD, exist_ok=True)
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
-    newest = max((os.path.getmtime(h) for h in _headers()), default=0.0)
     objs, todo = [], []
     for src in sources:
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(obj)
-        if _stale(obj, src, newest):
+        if _stale(obj, src):
             todo.append((src, obj))
+    # device-heavy translation units first, so that the longest compiles start at once
+    todo.sort(key=lambda so: (not so[0].endswith(".cu"), -os.path.getsize(so[0]) if "row_inst_32" not in so[0] else -1e9))
     if todo:
         with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 4)) as ex:
             for src, warn in ex.map(lambda so: _compile(so[0], so[1], verbose), todo):

@@ -98,7 +98,9 @@ AspbStatus finish_plan(sipfft::Plan &p, std::string (*builder)(sipfft::Plan &), 
 {
     p.steps.clear();
     p.tables.clear();
-    p.ws_buf_bytes[0] = p.ws_buf_bytes[1] = p.ws_buf_bytes[2] = 0;
+    p.c32_steps.clear();
+    p.c32_state = 0;
+    for (size_t &b : p.ws_buf_bytes) b = 0;
     if (builder != sipfft::build_plan_istft) p.istft = false;
     p.ws_bytes = 0;
     p.initialized = false;
@@ -137,10 +139,10 @@ AspbStatus finish_plan(sipfft::Plan &p, std::string (*builder)(sipfft::Plan &), 
 
 // Trailing-shape / dtype matching (fft_api.cpp:1047-1167) plus an element-count
 // check against the plan's batch.  kind: 0 complex full, 1 complex half, 2 real full.
-bool match_tensor(const sipfft::Plan &p, const aclTensor *t, int kind)
+bool match_tensor(const sipfft::Plan &p, const aclTensor *t, int kind, bool complex32 = false)
 {
     if (t == nullptr || t->data == nullptr) return false;
-    const aclDataType want = kind == 2 ? ACL_FLOAT : ACL_COMPLEX64;
+    const aclDataType want = kind == 2 ? ACL_FLOAT : (complex32 ? ACL_COMPLEX32 : ACL_COMPLEX64);
     if (t->dtype != want) return false;
     const auto &dims = t->view;
     int64_t expect = p.batch;
@@ -163,13 +165,19 @@ void *tensor_addr(const aclTensor *t)
 }
 
 AspbStatus run(sipfft::Plan &p, const void *in, void *out, const char *where, const float *in_im = nullptr,
-               float *out_im = nullptr)
+               float *out_im = nullptr, bool complex32 = false)
 {
     std::lock_guard<std::mutex> lock(p.mu);
     if (!p.initialized) {
         log_error(where, "plan is not initialised");
         return ACL_ERROR_INVALID_PARAM;
     }
+    if (complex32 && p.c32_state == 0) {
+        const std::string why = sipfft::complex32_steps(p, p.c32_steps);
+        p.c32_state = why.empty() ? 1 : -1;
+        if (!why.empty()) log_error(where, why.c_str());
+    }
+    if (complex32 && p.c32_state < 0) return ACL_ERROR_API_NOT_SUPPORT;
     if (p.ws_bytes > 0 && p.workspace == nullptr) {
         log_error(where, "workspace has not been set");
         return ACL_ERROR_INTERNAL_ERROR;
@@ -192,15 +200,17 @@ AspbStatus run(sipfft::Plan &p, const void *in, void *out, const char *where, co
             return ACL_ERROR_INVALID_PARAM;
         }
     }
-    const uintptr_t align_mask = p.fft_type == ASCEND_FFT_C2C_SEP ? 3 : 7;
+    const uintptr_t align_mask = (p.fft_type == ASCEND_FFT_C2C_SEP || complex32) ? 3 : 7;
     if ((reinterpret_cast<uintptr_t>(in) & align_mask) || (reinterpret_cast<uintptr_t>(out) & align_mask)) {
-        log_error(where, "device buffers must be 8-byte aligned");
+        log_error(where, complex32 ? "device buffers must be 4-byte aligned" : "device buffers must be 8-byte aligned");
         return ACL_ERROR_INVALID_PARAM;
     }
     int cur = 0;
     cudaGetDevice(&cur);
     if (cur != p.device) cudaSetDevice(p.device);
-    cudaError_t e = sipfft::execute_plan(p, in, out, static_cast<cudaStream_t>(p.stream), in_im, out_im);
+    cudaError_t e = complex32 ? sipfft::execute_steps(p, p.c32_steps, in, out, p.workspace,
+                                                      static_cast<cudaStream_t>(p.stream))
+                              : sipfft::execute_plan(p, in, out, static_cast<cudaStream_t>(p.stream), in_im, out_im);
     if (cur != p.device) cudaSetDevice(cur);
     if (e != cudaSuccess) {
         log_error(where, cudaGetErrorString(e));
@@ -505,11 +515,15 @@ AspbStatus asdFftExecC2C(asdFftHandle handle, const aclTensor *input, const aclT
     if (!p) return ACL_ERROR_INVALID_PARAM;
     if (p->istft) return ACL_ERROR_INVALID_PARAM;  // an ISTFT plan runs through asdFftExecIstft
     if (p->initialized && p->fft_type != ASCEND_FFT_C2C) return ACL_ERROR_INVALID_PARAM;
-    if (!match_tensor(*p, input, 0) || !match_tensor(*p, output, 0)) {
+    // complex32 in and out: the reference's FP16-complex DFT variant
+    // (ops/fft/c2c/dft/dft/kernel/dft_complex32.cpp:33, DftC32Kernel): FP16
+    // data, FP32 arithmetic
+    const bool c32 = input && output && input->dtype == ACL_COMPLEX32 && output->dtype == ACL_COMPLEX32;
+    if (!match_tensor(*p, input, 0, c32) || !match_tensor(*p, output, 0, c32)) {
         log_error("asdFftExecC2C", "input/output does not match plan");
         return ACL_ERROR_INVALID_PARAM;
     }
-    return run(*p, tensor_addr(input), tensor_addr(output), "asdFftExecC2C");
+    return run(*p, tensor_addr(input), tensor_addr(output), "asdFftExecC2C", nullptr, nullptr, c32);
 }
 
 AspbStatus asdFftExecC2R(asdFftHandle handle, const aclTensor *input, const aclTensor *output)

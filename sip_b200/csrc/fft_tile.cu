@@ -167,7 +167,7 @@ __device__ __forceinline__ void process_tile(const TileDesc &d, const void *in, 
         load_tile<FWD>(d, in, sm, o, c0, ntr);
         __syncthreads();
     }
-    const int64_t kc = loaded && d.g_twiddle ? (c0 + (thread_on ? l : 0)) % d.g_ns : -1;
+    const int64_t kc = loaded && d.g_twiddle ? pass_column(d, c0 + (thread_on ? l : 0)) : -1;
     if (flip) {
         conj_tile(d, sm, ntr);
         __syncthreads();
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(512, 1) tile_db_kernel(const __grid_constant__
         const int64_t c0 = (g % d.tiles_per_outer) * d.tb;
         const int64_t left = d.n_cols - c0;
         const int ntr = left < d.tb ? static_cast<int>(left) : d.tb;
-        const int64_t kc = d.g_twiddle ? (c0 + (thread_on ? l : 0)) % d.g_ns : -1;
+        const int64_t kc = d.g_twiddle ? pass_column(d, c0 + (thread_on ? l : 0)) : -1;
         run_stages<MAXE, FWD>(cur + (thread_on ? l : 0) * d.pitch, d, lane, thread_on && l < ntr, kc);
         store_tile<FWD>(d, d.out, cur, o, c0, ntr);
         __syncthreads();

@@ -87,6 +87,9 @@ struct TileDesc {
     int g_log2l;
     int64_t g_ns;
     int64_t g_step;    // F / (g_ns * n)
+    // Tile column c belongs to Stockham column c / g_div (a strided axis
+    // interleaves `inner` transforms per Stockham column); 0 or 1 = c itself.
+    int64_t g_div;
     const float2 *g_lo;
     const float2 *g_hi;
     // Per-stage twiddle tables of the compile-time (static) kernels: stage s
@@ -109,7 +112,17 @@ struct TileDesc {
     // Shared-memory buffers of a row kernel, each g_ns float2: 2 (double-
     // buffered tiles; 0 reads as 2) or 3 (plus a ping-pong work area).
     int row_bufs;
+    // complex32 (FP16 real / imaginary pairs) user data of a C2C step: bit 0 =
+    // the input, bit 1 = the output.  Loads widen to FP32, the stages run in
+    // FP32, stores round to FP16 (round to nearest even).
+    int half_io;
 };
+
+// Stockham column of tile column c for the pass twiddle: (c / g_div) mod g_ns.
+__host__ __device__ __forceinline__ int64_t pass_column(const TileDesc &d, int64_t c)
+{
+    return (d.g_div > 1 ? c / d.g_div : c) % d.g_ns;
+}
 
 // One segment of an uneven batch: a tile-kernel step whose source and
 // destination are byte offsets into one of four buffers (user input, user

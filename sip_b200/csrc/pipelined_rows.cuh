@@ -16,7 +16,7 @@
 // from the descriptor) or a compile-time StaticEngine (static_fft.cu).
 #pragma once
 #include "async_copy.cuh"
-#include "sipfft_internal.h"
+#include "fft_tile.cuh"
 #include "stages.cuh"
 
 namespace sipfft {

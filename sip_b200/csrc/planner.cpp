@@ -26,6 +26,8 @@ namespace {
 constexpr int64_t kMaxRowN = 16384;        // longest single-CTA transform: 512 threads x 32 points
 constexpr int64_t kMaxSingleTileC2C = 8192;  // longest C2C row planned as one tile
 constexpr int kMaxPassRadix = 2048;        // longest sub-FFT of one multi-pass Stockham pass
+constexpr int64_t kMaxStridedTile = 8192;  // longest strided axis planned as one column tile
+constexpr int64_t kMaxBluesteinM = int64_t(1) << 28;  // Bluestein for every N <= 2^27
 constexpr int kRowThreadsTarget = 256;     // threads per CTA for batched rows
 constexpr int kStaticRowThreads = 128;     // threads per CTA for rows on a compile-time engine
 constexpr int kRowSmemTarget = 64 * 1024;  // keep >= 3 CTAs per SM for short rows
@@ -178,14 +180,14 @@ struct Builder {
 
     void need_ws(Buf b, size_t bytes)
     {
-        const int i = b == Buf::kWs0 ? 0 : (b == Buf::kWs1 ? 1 : 2);
-        p.ws_buf_bytes[i] = std::max(p.ws_buf_bytes[i], bytes);
+        const int i = static_cast<int>(b) - static_cast<int>(Buf::kWs0);
+        if (i >= 0 && i < kWsSlots) p.ws_buf_bytes[i] = std::max(p.ws_buf_bytes[i], bytes);
     }
 
     // ASCEND_FFT_C2C_SEP: the C2C steps with separated real / imaginary user
     // planes.  The first step reads the planes, the last writes them; any
     // intermediate that the interleaved plan keeps in the user output (which
-    // holds only the real plane here) moves to workspace slot 2.
+    // holds only the real plane here) moves to workspace slot 3.
     bool make_planar()
     {
         const size_t S = p.steps.size();
@@ -202,10 +204,10 @@ struct Builder {
                 return false;
             }
             if (i + 1 < S && s.dst == Buf::kUserOut) {
-                s.dst = Buf::kWs2;
+                s.dst = Buf::kWs3;
                 redirect = true;
             }
-            if (i > 0 && s.src == Buf::kUserOut) s.src = Buf::kWs2;
+            if (i > 0 && s.src == Buf::kUserOut) s.src = Buf::kWs3;
             if (i > 0 && s.src == Buf::kUserIn) {
                 err = "separated layout: a later step reads the user input";
                 return false;
@@ -223,7 +225,7 @@ struct Builder {
             s.tc_fmt = -1;
             s.what += " [separated re/im]";
         }
-        if (redirect) need_ws(Buf::kWs2, size_t(elems) * sizeof(float2));
+        if (redirect) need_ws(Buf::kWs3, size_t(elems) * sizeof(float2));
         return true;
     }
 
@@ -443,16 +445,29 @@ struct Builder {
         }
     }
 
-    Buf other_ws(Buf a, Buf b)
+    // The first workspace slot that is none of `used` (slot 3 is kept for the
+    // planar redirect and only handed out when 0-2 are all taken).
+    Buf free_ws(std::initializer_list<Buf> used)
     {
-        if (a != Buf::kWs0 && b != Buf::kWs0) return Buf::kWs0;
-        if (a != Buf::kWs1 && b != Buf::kWs1) return Buf::kWs1;
-        return Buf::kWs0;
+        for (Buf c : {Buf::kWs0, Buf::kWs1, Buf::kWs2, Buf::kWs3}) {
+            bool taken = false;
+            for (Buf u : used) taken = taken || u == c;
+            if (!taken) return c;
+        }
+        return Buf::kWs3;
     }
+    Buf other_ws(Buf a, Buf b) { return free_ws({a, b}); }
 
-    // Multi-pass Stockham C2C of length F over `rows` contiguous rows.
-    // src rows have distance in_dist, dst rows out_dist (complex units).
-    bool add_multipass(int64_t F, int64_t rows, int64_t in_dist, int64_t out_dist, Buf src, Buf dst)
+    // Multi-pass Stockham C2C of length F along one axis of [outer][F][inner]
+    // (inner = 1: contiguous rows; src rows at in_dist, dst rows at out_dist
+    // complex elements).  Pass i is a column-tile launch over the F / R_i
+    // Stockham columns of every transform: tile column C = c * inner + j is
+    // Stockham column c of transform j, so a tile of consecutive C reads
+    // consecutive addresses whenever inner > 1.  The pass twiddle W_F^(r c ns)
+    // comes from the two-level table; intermediates go to workspace slots that
+    // are neither src nor dst.
+    bool add_multipass(int64_t F, int64_t outer, int64_t in_dist, int64_t out_dist, Buf src, Buf dst,
+                       int64_t inner = 1)
     {
         std::vector<int> passes;
         int parts = 2;
@@ -472,18 +487,20 @@ struct Builder {
             const int rp = passes[i];
             const bool last = i + 1 == passes.size();
             Buf nxt = last ? dst : other_ws(cur, dst);
-            const int64_t nxt_dist = last ? out_dist : F;
-            if (!last) need_ws(nxt, size_t(rows) * F * sizeof(float2));
+            const int64_t nxt_dist = last ? out_dist : F * inner;
+            if (!last) need_ws(nxt, size_t(outer) * F * inner * sizeof(float2));
             const float2 *tw = table(rp, rp);
             if (!tw) return false;
-            Addr ia{cur_dist, 1, F / rp, 0, 0};
-            Addr oa{nxt_dist, 1, ns, ns, ns * (rp - 1)};
+            Addr ia{cur_dist, 1, (F / rp) * inner, 0, 0};
+            Addr oa{nxt_dist, 1, ns * inner, ns * inner, ns * inner * (rp - 1)};
             std::ostringstream w;
             w << "pass " << i << " radix " << rp << " of " << F << " (Ns=" << ns << ")";
-            if (!add_tile(IO_C2C, rp, 1, tw, true, rows, F / rp, ia, oa, cur, nxt, w.str())) return false;
+            if (inner > 1) w << " strided x" << inner;
+            if (!add_tile(IO_C2C, rp, 1, tw, true, outer, (F / rp) * inner, ia, oa, cur, nxt, w.str())) return false;
             TileDesc &d = p.steps.back().d;
             d.g_twiddle = ns > 1 ? 1 : 0;
             d.g_ns = ns;
+            d.g_div = inner;
             d.g_step = F / (ns * rp);
             d.g_lo = lo;
             d.g_hi = hi;
@@ -504,10 +521,11 @@ struct Builder {
     {
         int64_t m = 1;
         while (m < 2 * n - 1) m *= 2;
-        if (m > kMaxRowN) {
-            err = "length " + std::to_string(n) + " needs Bluestein with M > " + std::to_string(kMaxRowN);
+        if (m > kMaxBluesteinM) {
+            err = "length " + std::to_string(n) + " needs Bluestein with M > " + std::to_string(kMaxBluesteinM);
             return false;
         }
+        const bool multipass = m > kMaxRowN;
         auto chirp = std::make_shared<DeviceTable>();
         auto bmul = std::make_shared<DeviceTable>();
         chirp->device = bmul->device = device;
@@ -517,9 +535,11 @@ struct Builder {
         if (e == cudaSuccess) e = cudaMalloc(&bmul->ptr, sizeof(float2) * m);
         if (e == cudaSuccess) e = fill_chirp(chirp->ptr, n, fwd, 0);
         if (e == cudaSuccess) e = fill_bluestein_b(bmul->ptr, chirp->ptr, n, m, 0);
-        const float2 *twm = table(m, m);
-        if (!twm) return false;
-        if (e == cudaSuccess) {
+        const float2 *twm = multipass ? nullptr : table(m, m);
+        if (!multipass && !twm) return false;
+        if (e == cudaSuccess && multipass) {
+            e = fft_in_place_once(bmul->ptr, m);
+        } else if (e == cudaSuccess) {
             // FFT_M of b in place (one row, forward), then fold in the 1/M of the inverse
             Step tmp;
             if (!make_tile(tmp, IO_C2C, static_cast<int>(m), 1, twm, false, 1, 1, Addr{0, m, 1, 0, 0},
@@ -538,6 +558,7 @@ struct Builder {
         }
         p.tables.push_back(chirp);
         p.tables.push_back(bmul);
+        if (multipass) return add_bluestein_steps(kind, n, m, rows, in_dist, out_dist, src, dst, chirp->ptr, bmul->ptr);
         Buf ws = other_ws(src, dst);
         need_ws(ws, size_t(rows) * m * sizeof(float2));
         std::ostringstream w;
@@ -559,6 +580,76 @@ struct Builder {
         s2.forward = false;
         p.steps.push_back(s1);
         p.steps.push_back(s2);
+        return true;
+    }
+
+    // Forward FFT of one length-m row in place at plan time (the Bluestein
+    // filter of a multi-pass convolution): a one-row plan of this planner run
+    // with a temporary workspace.
+    cudaError_t fft_in_place_once(float2 *row, int64_t m)
+    {
+        Plan tmp;
+        tmp.device = device;
+        tmp.fft_type = 0x10;
+        tmp.direction = 0x10;
+        tmp.sizes = {m};
+        tmp.batch = 1;
+        const std::string why = build_plan_1d(tmp);
+        if (!why.empty()) return cudaErrorInvalidValue;
+        void *ws = nullptr;
+        cudaError_t e = tmp.ws_bytes ? cudaMalloc(&ws, tmp.ws_bytes) : cudaSuccess;
+        if (e == cudaSuccess) e = execute_steps(tmp, tmp.steps, row, row, ws, 0);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+        if (ws) cudaFree(ws);
+        return e;
+    }
+
+    // Bluestein with a convolution length m too long for one CTA: chirp
+    // multiply into workspace A, forward multi-pass FFT A -> B, pointwise
+    // product with the transformed filter, inverse multi-pass FFT B -> A, chirp
+    // multiply into the destination.
+    bool add_bluestein_steps(int kind, int64_t n, int64_t m, int64_t rows, int64_t in_dist, int64_t out_dist, Buf src,
+                             Buf dst, const float2 *chirp, const float2 *bmul)
+    {
+        const Buf A = free_ws({src, dst}), B = free_ws({src, dst, A});
+        need_ws(A, size_t(rows) * m * sizeof(float2));
+        need_ws(B, size_t(rows) * m * sizeof(float2));
+        std::ostringstream w;
+        w << "Bluestein n=" << n << " via M=" << m << " rows=" << rows << " (multi-pass)";
+        Step pre;
+        pre.kind = StepKind::kBluePre;
+        pre.src = src;
+        pre.dst = A;
+        pre.rows = rows;
+        pre.m = m;
+        pre.src_dist = in_dist;
+        pre.d.blue_n = static_cast<int>(n);
+        pre.d.blue_kind = kind;
+        pre.d.chirp = chirp;
+        pre.what = w.str() + ": chirp multiply";
+        p.steps.push_back(pre);
+        const bool plan_fwd = fwd;
+        fwd = true;
+        bool ok = add_multipass(m, rows, m, m, A, B);
+        if (ok) {
+            Step mul = pre;
+            mul.kind = StepKind::kPointMul;
+            mul.src = mul.dst = B;
+            mul.d.bmul = bmul;
+            mul.what = w.str() + ": filter product";
+            p.steps.push_back(mul);
+            fwd = false;
+            ok = add_multipass(m, rows, m, m, B, A);
+        }
+        fwd = plan_fwd;
+        if (!ok) return false;
+        Step post = pre;
+        post.kind = StepKind::kBluePost;
+        post.src = A;
+        post.dst = dst;
+        post.dst_dist = out_dist;
+        post.what = w.str() + ": chirp multiply";
+        p.steps.push_back(post);
         return true;
     }
 
@@ -586,10 +677,17 @@ struct Builder {
             }
             return add_multipass(n, outer, n, n, src, dst);
         }
-        TileCfg c;
-        if (n > 32768 || !choose_cfg(static_cast<int>(n), true, inner, c, err)) {
-            err = "strided axis of length " + std::to_string(n) + " is not supported";
+        if (!smooth) {
+            err = "strided axis of length " + std::to_string(n) + " has a prime factor above 13";
             return false;
+        }
+        TileCfg c;
+        if (n > kMaxStridedTile || !choose_cfg(static_cast<int>(n), true, inner, c, err)) {
+            // longer strided axes: multi-pass Stockham with 16-column tiles along the
+            // contiguous inner dimension (the reference's stride core plans powers of
+            // two up to 262144, core/fft/fftcore/fft_core_stride.cpp:119-161)
+            err.clear();
+            return add_multipass(n, outer, n * inner, n * inner, src, dst, inner);
         }
         const float2 *tw = table(n, n);
         if (!tw) return false;
@@ -710,10 +808,7 @@ std::string finish(Plan &p, Builder &b, bool ok)
         return b.err;
     }
     p.ws_bytes = 0;
-    if (p.ws_buf_bytes[0] || p.ws_buf_bytes[1] || p.ws_buf_bytes[2]) {
-        auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-        p.ws_bytes = al(p.ws_buf_bytes[0]) + al(p.ws_buf_bytes[1]) + al(p.ws_buf_bytes[2]);
-    }
+    for (size_t b : p.ws_buf_bytes) p.ws_bytes += (b + 255) / 256 * 256;
     return std::string();
 }
 

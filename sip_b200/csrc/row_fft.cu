@@ -1,35 +1,32 @@
-// Runtime-radix instantiation of the TMA-pipelined row kernel
-// (pipelined_rows.cuh) and its host-side launch helpers.
+// Runtime-radix TMA-pipelined row kernels (pipelined_rows.cuh, instantiated in
+// row_inst_*.cu) and their host-side launch helpers.
 #include <vector>
 
-#include "pipelined_rows.cuh"
+#include "row_fft_inst.cuh"
+#include "sipfft_internal.h"
 
 namespace sipfft {
 
 namespace {
 
-template <int MAXE, bool FWD, int IO>
-const void *row_fn()
+const void *row_fn_io8(bool forward, int io)
 {
-    return reinterpret_cast<const void *>(pipelined_rows_kernel<RuntimeEngine<MAXE>, FWD, IO>);
+    return forward ? runtime_row_kernel_8_fwd(io) : runtime_row_kernel_8_inv(io);
 }
-
-template <int MAXE, bool FWD>
-const void *row_fn_io(int io)
+const void *row_fn_io16(bool forward, int io)
 {
-    switch (io) {
-        case IO_C2C: return row_fn<MAXE, FWD, IO_C2C>();
-        case IO_R2C_PACKED: return row_fn<MAXE, FWD, IO_R2C_PACKED>();
-        case IO_C2R_PACKED: return row_fn<MAXE, FWD, IO_C2R_PACKED>();
-        default: return nullptr;
-    }
+    return forward ? runtime_row_kernel_16_fwd(io) : runtime_row_kernel_16_inv(io);
+}
+const void *row_fn_io32(bool forward, int io)
+{
+    return forward ? runtime_row_kernel_32_fwd(io) : runtime_row_kernel_32_inv(io);
 }
 
 const void *pick(const TileDesc &d, int maxe, bool forward)
 {
-    if (maxe <= 8) return forward ? row_fn_io<8, true>(d.io) : row_fn_io<8, false>(d.io);
-    if (maxe <= 16) return forward ? row_fn_io<16, true>(d.io) : row_fn_io<16, false>(d.io);
-    return forward ? row_fn_io<32, true>(d.io) : row_fn_io<32, false>(d.io);
+    if (maxe <= 8) return row_fn_io8(forward, d.io);
+    if (maxe <= 16) return row_fn_io16(forward, d.io);
+    return row_fn_io32(forward, d.io);
 }
 
 }  // namespace
@@ -74,12 +71,11 @@ cudaError_t launch_kernel_fn(const void *fn, const TileDesc &d, int grid, size_t
 void row_kernel_fns(std::vector<const void *> &out)
 {
     for (int io : {IO_C2C, IO_R2C_PACKED, IO_C2R_PACKED}) {
-        out.push_back(row_fn_io<8, true>(io));
-        out.push_back(row_fn_io<8, false>(io));
-        out.push_back(row_fn_io<16, true>(io));
-        out.push_back(row_fn_io<16, false>(io));
-        out.push_back(row_fn_io<32, true>(io));
-        out.push_back(row_fn_io<32, false>(io));
+        for (bool f : {true, false}) {
+            out.push_back(row_fn_io8(f, io));
+            out.push_back(row_fn_io16(f, io));
+            out.push_back(row_fn_io32(f, io));
+        }
     }
 }
 

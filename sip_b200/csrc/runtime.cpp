@@ -183,6 +183,33 @@ int sm_count(int device)
     return n;
 }
 
+std::string complex32_steps(const Plan &p, std::vector<Step> &out)
+{
+    if (p.fft_type != 0x10 || p.sizes.size() != 1) return "complex32 data is supported for 1D C2C plans";
+    if (p.precision != 0) return "complex32 data runs with FP32 stages only (precision mode 0)";
+    out = p.steps;
+    if (out.empty()) return "empty plan";
+    for (size_t i = 0; i < out.size(); i++) {
+        Step &s = out[i];
+        if (s.kind != StepKind::kTile || s.d.io != IO_C2C || s.d.planar)
+            return "complex32 data needs a plan of C2C tile steps (no Bluestein lengths)";
+        if ((i == 0) != (s.src == Buf::kUserIn) || (i + 1 == out.size()) != (s.dst == Buf::kUserOut) ||
+            s.src == Buf::kUserOut)
+            return "complex32 data needs the user buffers to be read first and written last only";
+    }
+    for (Step *s : {&out.front(), &out.back()}) {
+        // the first / last step run on the generic tile kernel, whose load and
+        // store phases convert
+        s->has_row = false;
+        s->row_fn = nullptr;
+        s->db = false;
+        s->db_fn = nullptr;
+    }
+    out.front().d.half_io |= 1;
+    out.back().d.half_io |= 2;
+    return std::string();
+}
+
 // Copy of a 1D row plan's steps re-targeted to `rows` (<= the planned
 // batch) transforms, so one resident plan serves batches of any size.
 bool scale_steps_to_rows(const Plan &p, int64_t rows, std::vector<Step> &out)
@@ -226,9 +253,12 @@ cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const v
                           cudaStream_t st, const float *in_im, float *out_im)
 {
     char *ws = static_cast<char *>(workspace);
-    const size_t off1 = (p.ws_buf_bytes[0] + 255) / 256 * 256;
-    const size_t off2 = off1 + (p.ws_buf_bytes[1] + 255) / 256 * 256;
-    void *bufs[5] = {const_cast<void *>(in), out, ws, ws ? ws + off1 : nullptr, ws ? ws + off2 : nullptr};
+    void *bufs[2 + kWsSlots] = {const_cast<void *>(in), out};
+    size_t off = 0;
+    for (int i = 0; i < kWsSlots; i++) {
+        bufs[2 + i] = ws ? ws + off : nullptr;
+        off += (p.ws_buf_bytes[i] + 255) / 256 * 256;
+    }
     for (const Step &s : steps) {
         const void *src = bufs[static_cast<int>(s.src)];
         void *dst = bufs[static_cast<int>(s.dst)];
@@ -284,6 +314,17 @@ cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const v
             case StepKind::kC2RPre:
                 e = launch_c2r_pre(static_cast<const float2 *>(src), static_cast<float2 *>(dst), s.rows, s.m,
                                    s.src_dist, s.dst_dist, s.lo, s.hi, s.log2l, s.forward, st);
+                break;
+            case StepKind::kBluePre:
+                e = launch_blue_pre(src, static_cast<float2 *>(dst), s.rows, s.d.blue_n, s.m, s.src_dist,
+                                    s.d.blue_kind, s.d.chirp, st);
+                break;
+            case StepKind::kPointMul:
+                e = launch_point_mul(static_cast<float2 *>(dst), s.d.bmul, s.rows, s.m, st);
+                break;
+            case StepKind::kBluePost:
+                e = launch_blue_post(static_cast<const float2 *>(src), dst, s.rows, s.d.blue_n, s.m, s.dst_dist,
+                                     s.d.blue_kind, s.d.chirp, st);
                 break;
         }
         if (e != cudaSuccess) return e;

@@ -106,6 +106,16 @@ cudaError_t launch_r2c_post(const float2 *z, float2 *x, int64_t rows, int64_t m,
                             const float2 *tw_lo, const float2 *tw_hi, int log2l, bool forward, cudaStream_t st);
 cudaError_t launch_c2r_pre(const float2 *x, float2 *z, int64_t rows, int64_t m, int64_t xdist, int64_t zdist,
                            const float2 *tw_lo, const float2 *tw_hi, int log2l, bool forward, cudaStream_t st);
+// Element-wise Bluestein stages for multi-pass convolution lengths (fft_aux.cu):
+// a[r][e] = x_r[e] chirp[e] (e < n, else 0) over rows of m; b[r][e] *= bmul[e];
+// y_r[k] = chirp[k] a[r][k] for the first n (kind 1: n/2+1; kind 2: real part of n).
+// kind: 0 complex, 1 real input / half-spectrum output, 2 Hermitian half-spectrum
+// input / real output.
+cudaError_t launch_blue_pre(const void *in, float2 *a, int64_t rows, int64_t n, int64_t m, int64_t in_dist, int kind,
+                            const float2 *chirp, cudaStream_t st);
+cudaError_t launch_point_mul(float2 *b, const float2 *bmul, int64_t rows, int64_t m, cudaStream_t st);
+cudaError_t launch_blue_post(const float2 *a, void *out, int64_t rows, int64_t n, int64_t m, int64_t out_dist,
+                             int kind, const float2 *chirp, cudaStream_t st);
 
 // A device twiddle table shared between plans (the reference's FFTensorCache,
 // core/fft/utils/fftensor_cache.cpp:55-92, keeps coefficient tensors alive
@@ -130,9 +140,16 @@ TablePtr get_stage_table(const int *radix, int nstages, int device, std::string 
 // ptr, lo at ptr + N^2 float2, each 2N x 2N 16-bit values.
 TablePtr get_tc_matrix(int N, int fmt, bool fwd, int device, std::string *err, int layout = 0);
 
-enum class Buf : int { kUserIn = 0, kUserOut = 1, kWs0 = 2, kWs1 = 3, kWs2 = 4 };
+// Buffers a step reads or writes: the caller's input and output, and four
+// slots of the caller's workspace (kWs3 holds the intermediates that a planar
+// plan moves out of the caller's output).
+enum class Buf : int { kUserIn = 0, kUserOut = 1, kWs0 = 2, kWs1 = 3, kWs2 = 4, kWs3 = 5 };
+constexpr int kWsSlots = 4;
 
-enum class StepKind : int { kTile = 0, kR2CPost = 1, kC2RPre = 2 };
+// kBluePre / kPointMul / kBluePost: the element-wise stages of a Bluestein
+// transform whose convolution length M is too long for one CTA (the M-point
+// FFTs between them are multi-pass tile steps).
+enum class StepKind : int { kTile = 0, kR2CPost = 1, kC2RPre = 2, kBluePre = 3, kPointMul = 4, kBluePost = 5 };
 
 struct Step {
     StepKind kind = StepKind::kTile;
@@ -186,7 +203,7 @@ struct Plan {
     // build-specific
     int device = 0;
     std::vector<Step> steps;
-    size_t ws_buf_bytes[3] = {0, 0, 0};
+    size_t ws_buf_bytes[kWsSlots] = {0, 0, 0, 0};
     size_t ws_bytes = 0;
     std::vector<TablePtr> tables;
     std::mutex mu;
@@ -202,6 +219,10 @@ struct Plan {
     // 0: FP32 kernels; 1: tensor-core FP16 hi/lo x3; 2: tensor-core BF16 hi/lo x3
     // (lengths without a tensor-core stage keep the FP32 kernels)
     int precision = 0;
+    // complex32 (FP16 pairs) variant of a 1D C2C plan's steps, built at the
+    // first complex32 exec (c32_state: 0 not built, 1 built, -1 unsupported)
+    std::vector<Step> c32_steps;
+    int c32_state = 0;
     bool forward() const;
 };
 
@@ -225,6 +246,10 @@ cudaError_t execute_plan(Plan &p, const void *in, void *out, cudaStream_t st, co
 cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const void *in, void *out, void *workspace,
                           cudaStream_t st, const float *in_im = nullptr, float *out_im = nullptr);
 bool scale_steps_to_rows(const Plan &p, int64_t rows, std::vector<Step> &out);
+// Copy of a 1D C2C plan's steps that reads and writes complex32 user data
+// (the first step widens on load, the last rounds on store, FP32 in between).
+// Empty string on success, else why the plan has no complex32 form.
+std::string complex32_steps(const Plan &p, std::vector<Step> &out);
 std::string describe_plan(const Plan &p);
 
 // Radix decomposition used by the tile kernel (largest radices first).

@@ -8,6 +8,7 @@
 // engines plug into the TMA-pipelined row skeleton (pipelined_rows.cuh).
 // Lengths without a specialisation use the runtime-radix engine.
 #include "pipelined_rows.cuh"
+#include "sipfft_internal.h"
 #include "tile_io.cuh"
 
 namespace sipfft {
@@ -521,7 +522,7 @@ __global__ void __launch_bounds__(512, 1) static_db_kernel(const __grid_constant
         float2 *row = cur + (thread_on ? l : 0) * d.pitch;
         const bool act = thread_on && l < ntr;
         if (d.g_twiddle) {
-            const int64_t kc = (c0 + (thread_on ? l : 0)) % d.g_ns;
+            const int64_t kc = pass_column(d, c0 + (thread_on ? l : 0));
             E::template run<FWD>(d, row, PassRow<FWD>{row, &d, kc}, SmemRow{row}, true, lane, act);
         } else {
             E::template run<FWD>(d, row, SmemRow{row}, SmemRow{row}, true, lane, act);

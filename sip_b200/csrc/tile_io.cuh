@@ -3,6 +3,8 @@
 // Shared by the SIMT tile kernel (fft_tile.cu) and the tensor-core kernel
 // (tc_fft.cu).  The shared-memory row index is padded (pad(i) = i + i/16).
 #pragma once
+#include <cuda_fp16.h>
+
 #include "async_copy.cuh"
 #include "codelets.cuh"
 #include "fft_tile.cuh"
@@ -124,7 +126,7 @@ __device__ __forceinline__ void load_tile(const TileDesc &d, const void *in, flo
         const float *xr = static_cast<const float *>(in) + base;
         const float *xi = d.in_im + base;
         if (d.g_twiddle) {
-            const int64_t kc = (c0 + l) % d.g_ns;
+            const int64_t kc = pass_column(d, c0 + l);
             for (int e = e0; e < n; e += estep)
                 row[pad(e)] = cmul(make_float2(xr[e * es], xi[e * es]), pass_twiddle<FWD>(d, e, kc));
         } else {
@@ -137,9 +139,15 @@ __device__ __forceinline__ void load_tile(const TileDesc &d, const void *in, flo
         for (int e = e0; e < n; e += estep) row[pad(e)] = make_float2(x[e * es], 0.f);
         return;
     }
+    if (d.half_io & 1) {
+        // complex32 input (first step of a C2C plan, no pass twiddle)
+        const __half2 *xh = static_cast<const __half2 *>(in) + base;
+        for (int e = e0; e < n; e += estep) row[pad(e)] = __half22float2(xh[e * es]);
+        return;
+    }
     const float2 *x = static_cast<const float2 *>(in) + base;
     if (d.g_twiddle) {
-        const int64_t kc = (c0 + l) % d.g_ns;
+        const int64_t kc = pass_column(d, c0 + l);
         for (int e = e0; e < n; e += estep) row[pad(e)] = cmul(x[e * es], pass_twiddle<FWD>(d, e, kc));
     } else {
         for (int e = e0; e < n; e += estep) row[pad(e)] = x[e * es];
@@ -225,6 +233,12 @@ __device__ __forceinline__ void store_tile(const TileDesc &d, void *out, const f
     if (io == IO_C2R_FULL) {
         float *y = static_cast<float *>(out) + base;
         for (int e = e0; e < n; e += estep) y[e * es] = row[pad(e)].x;
+        return;
+    }
+    if (d.half_io & 2) {
+        // complex32 output (last step of a C2C plan)
+        __half2 *yh = static_cast<__half2 *>(out) + base;
+        for (int e = e0; e < n; e += estep) yh[e * es] = __float22half2_rn(row[pad(e)]);
         return;
     }
     const int count = (io == IO_R2C_FULL) ? n / 2 + 1 : n;

@@ -51,6 +51,7 @@ PRECISION_BF16X3 = 2     # the same with BF16 hi/lo parts
 
 ACL_FLOAT = 0
 ACL_COMPLEX64 = 16
+ACL_COMPLEX32 = 33  # FP16 real / imaginary pairs (CANN aclDataType)
 ACL_FORMAT_ND = 2
 
 # every exported symbol the public headers declare

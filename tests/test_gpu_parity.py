@@ -75,8 +75,8 @@ def check(sizes, typ, fwd, batch, seed=0, vertical=False):
 
 C2C_SIZES = [1, 2, 3, 4, 5, 7, 8, 11, 13, 16, 30, 64, 100, 128, 143, 210, 256, 343, 512, 1000, 1024, 1500,
              2048, 3000, 4096, 6561, 8192, 10000, 15000, 16384, 24576, 32768, 65536, 3 * 2 ** 15, 2 ** 20,
-             # prime factors above 13: Bluestein
-             17, 31, 97, 202, 1021, 4099, 8191]
+             # prime factors above 13: Bluestein (single-tile convolution up to M = 16384, multi-pass above)
+             17, 31, 97, 202, 1021, 4099, 8191, 17 * 1024, 199 * 1000, 65537, 199 * 199 * 13]
 
 
 @pytest.mark.parametrize("n", C2C_SIZES)
@@ -88,8 +88,9 @@ def test_c2c_1d(cuda, n, fwd):
 
 REAL_SIZES = [1, 2, 3, 4, 5, 6, 7, 30, 64, 100, 243, 256, 1000, 1024, 3000, 4096, 8192, 15625, 16384,
               30000, 65536, 131072,
-              # prime factors above 13 (Bluestein): odd, even, and even with an odd large half
-              17, 31, 34, 1021, 2042]
+              # prime factors above 13 (Bluestein): odd, even, and even with an odd large half;
+              # multi-pass convolutions for the long ones
+              17, 31, 34, 1021, 2042, 17 * 1024, 199 * 1000, 2 * 65537, 65537]
 
 
 @pytest.mark.parametrize("n", REAL_SIZES)
@@ -100,10 +101,20 @@ def test_real_1d(cuda, n, fwd, typ):
     check([n], typ, fwd, batch, seed=n + typ)
 
 
-@pytest.mark.parametrize("n,batch", [(256, 128), (1024, 200), (60, 33), (4096, 16)])
+@pytest.mark.parametrize("n,batch", [(256, 128), (1024, 200), (60, 33), (4096, 16),
+                                     # long strided axes: multi-pass column tiles (the reference's
+                                     # vertical 1D takes powers of two up to 65536)
+                                     (16384, 128), (65536, 128), (3 * 5 * 7 * 1024, 16), (262144, 16)])
 @pytest.mark.parametrize("fwd", [FWD, INV])
 def test_c2c_vertical(cuda, n, batch, fwd):
     check([n], C2C, fwd, batch, seed=n, vertical=True)
+
+
+@pytest.mark.parametrize("shape,typ", [((65536, 4), C2C), ((16384, 8), C2C), ((32768, 6), R2C), ((32768, 6), C2R),
+                                       ((4, 16384, 8), C2C)])
+def test_long_strided_axes(cuda, shape, typ):
+    """2D / 3D plans whose strided (leading) axes are too long for one column tile."""
+    check(list(shape), typ, FWD, 2, seed=int(np.prod(shape)))
 
 
 SIZES_2D = [(1, 1), (3, 5), (32, 32), (64, 128), (100, 60), (2, 4096), (2048, 2048)]
@@ -221,9 +232,13 @@ def test_exec_error_paths(cuda):
     y = torch.zeros((1, 65536), dtype=torch.complex64, device="cuda")
     assert fft.load_library().asdFftExecRaw(h, y.data_ptr(), y.data_ptr()) == fft.ACL_ERROR_INTERNAL_ERROR
     assert fft.asdFftDestroy(h) == fft.ACL_SUCCESS
-    # an unsupported length (large prime beyond the Bluestein range) is refused at plan time
+    # lengths above the reference's limit (2^27) are refused at plan time
     h = fft.asdFftCreate()
-    assert fft.asdFftMakePlan1D(h, 65537, C2C, FWD, 1) == fft.ACL_ERROR_API_NOT_SUPPORT
+    assert fft.asdFftMakePlan1D(h, 2 ** 27 + 1, C2C, FWD, 1) == fft.ACL_ERROR_INVALID_PARAM
+    fft.asdFftDestroy(h)
+    # a strided axis with a prime factor above 13 is not planned
+    h = fft.asdFftCreate()
+    assert fft.asdFftMakePlan2D(h, 17, 64, C2C, FWD, 1) == fft.ACL_ERROR_API_NOT_SUPPORT
     fft.asdFftDestroy(h)
 
 
@@ -287,4 +302,62 @@ def test_pipelined_and_generic_kernels_agree(cuda, typ, n):
         assert oracle.rel_l2(outs[-1], ref) <= oracle.tolerance(n)
     assert np.max(np.abs(outs[0] - outs[1])) <= 1e-6 * np.max(np.abs(ref))
     assert fft.asdFftSynchronize(plan.handle) == fft.ACL_SUCCESS
+    plan.close()
+
+
+@pytest.mark.parametrize("n,batch", [(64, 33), (256, 16), (1000, 8), (4096, 4), (65536, 2)])
+@pytest.mark.parametrize("fwd", [FWD, INV])
+def test_complex32_c2c(cuda, n, batch, fwd):
+    """complex32 (FP16 pairs) in and out of a C2C plan, FP32 arithmetic: the
+    reference's DftC32Kernel variant (ops/fft/c2c/dft/dft/kernel/dft_complex32.cpp).
+    The result equals the FP32 path's output rounded to FP16 (to one FP16 ulp)
+    and is within FP16 output rounding of the FP64 oracle."""
+    import torch
+
+    rng = np.random.default_rng(n + fwd)
+    x = _rand_complex(rng, (batch, n)).astype(np.complex64)
+    xh = np.stack([x.real, x.imag], axis=-1).astype(np.float16)     # [batch, n, 2]
+    xd = torch.from_numpy(xh).cuda()
+    yd = torch.full_like(xd, float("nan"))
+    plan = fft.FftPlan([n], C2C, fwd, batch)
+    a = fft.AclTensor([batch, n], fft.ACL_COMPLEX32, xd.data_ptr())
+    b = fft.AclTensor([batch, n], fft.ACL_COMPLEX32, yd.data_ptr())
+    assert fft.asdFftExecC2C(plan.handle, a, b) == fft.ACL_SUCCESS
+    torch.cuda.synchronize()
+    y = yd.cpu().numpy().astype(np.float64)
+    got = y[..., 0] + 1j * y[..., 1]
+    xin = xh.astype(np.float64)
+    ref = oracle.c2c(xin[..., 0] + 1j * xin[..., 1], fwd == FWD)
+    assert np.all(np.isfinite(got))
+    assert oracle.rel_l2(got, ref) <= 1e-3, oracle.rel_l2(got, ref)
+    # the FP32 path on the same (FP16-exact) input, rounded to FP16
+    xc = torch.from_numpy((xin[..., 0] + 1j * xin[..., 1]).astype(np.complex64)).cuda()
+    y32 = torch.empty_like(xc)
+    plan(xc, y32)
+    torch.cuda.synchronize()
+    r = torch.view_as_real(y32).half().float().cpu().numpy()
+    ulp = np.abs(np.spacing(r.astype(np.float16)).astype(np.float64))
+    assert np.all(np.abs(y - r) <= ulp + 1e-30)
+    # in place
+    assert fft.asdFftExecC2C(plan.handle, a, a) == fft.ACL_SUCCESS
+    torch.cuda.synchronize()
+    assert np.array_equal(xd.cpu().numpy(), yd.cpu().numpy())
+    a.close()
+    b.close()
+    plan.close()
+
+
+def test_complex32_refused_where_unsupported(cuda):
+    import torch
+
+    x = torch.zeros((4, 64, 64, 2), dtype=torch.float16, device="cuda")
+    plan = fft.FftPlan([64, 64], C2C, FWD, 4)
+    a = fft.AclTensor([4, 64, 64], fft.ACL_COMPLEX32, x.data_ptr())
+    assert fft.asdFftExecC2C(plan.handle, a, a) == fft.ACL_ERROR_API_NOT_SUPPORT   # 2D
+    a.close()
+    plan.close()
+    plan = fft.FftPlan([17], C2C, FWD, 4)  # Bluestein length
+    a = fft.AclTensor([4, 17], fft.ACL_COMPLEX32, x.data_ptr())
+    assert fft.asdFftExecC2C(plan.handle, a, a) == fft.ACL_ERROR_API_NOT_SUPPORT
+    a.close()
     plan.close()
