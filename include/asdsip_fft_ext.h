@@ -33,8 +33,8 @@ ASDSIP_API int32_t asdFftPlanLaunchCount(void *handle);
  * mode 1: tensor-core (tcgen05) DFT-matrix stages, operands split into FP16 hi + lo parts with a
  *         power-of-two scale per tile, three products hi*hi + hi*lo + lo*hi accumulated in FP32.
  * mode 2: the same with BF16 hi + lo parts (no scaling; about 16 significant bits per operand).
- * Tensor-core stages exist for transform lengths 1024, 2048 and 4096 of a C2C axis (and 2048, 4096 and
- * 8192 for R2C / C2R, whose packed inner transform has half the length); every other step keeps the FP32
+ * Tensor-core stages exist for transform lengths 256, 1024, 2048 and 4096 of a C2C axis (and 512, 2048,
+ * 4096 and 8192 for R2C / C2R, whose packed inner transform has half the length); every other step keeps the FP32
  * kernels, which asdFftDescribePlan shows.  May be called before or after MakePlan*: an initialised
  * plan is rebuilt (the workspace size does not change).  Returns ACL_ERROR_INVALID_PARAM for an unknown
  * handle or mode. */

@@ -359,6 +359,7 @@ const void *tc_fn(bool fwd)
 bool tc_config(int n, TcConfig &c)
 {
     switch (n) {
+        case 256: c = {16, 16, 8}; return true;
         case 1024: c = {32, 32, 4}; return true;
         case 2048: c = {64, 32, 2}; return true;
         case 4096: c = {64, 64, 1}; return true;
@@ -373,6 +374,7 @@ const void *tc_kernel(int n, int fmt, bool fwd, size_t *smem)
         if (smem) *smem = fmt == 0 ? TcShape<A, B, T, 0, true>::SMEM : TcShape<A, B, T, 1, true>::SMEM; \
         return fmt == 0 ? tc_fn<A, B, T, 0>(fwd) : tc_fn<A, B, T, 1>(fwd);                \
     }
+    SIPFFT_TC(256, 16, 16, 8)
     SIPFFT_TC(1024, 32, 32, 4)
     SIPFFT_TC(2048, 64, 32, 2)
     SIPFFT_TC(4096, 64, 64, 1)
@@ -382,7 +384,7 @@ const void *tc_kernel(int n, int fmt, bool fwd, size_t *smem)
 
 void tc_kernel_fns(std::vector<const void *> &out)
 {
-    for (int n : {1024, 2048, 4096})
+    for (int n : {256, 1024, 2048, 4096})
         for (int fmt = 0; fmt < 2; fmt++)
             for (int f = 0; f < 2; f++) out.push_back(tc_kernel(n, fmt, f != 0, nullptr));
 }

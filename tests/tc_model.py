@@ -13,7 +13,7 @@ from __future__ import annotations
 
 import numpy as np
 
-CONFIGS = {1024: (32, 32, 4), 2048: (64, 32, 2), 4096: (64, 64, 1)}
+CONFIGS = {256: (16, 16, 8), 1024: (32, 32, 4), 2048: (64, 32, 2), 4096: (64, 64, 1)}
 SMEM_LIMIT = 227 * 1024
 TMEM_COLS = 128
 

@@ -336,8 +336,10 @@ def test_complex32_c2c(cuda, n, batch, fwd):
     plan(xc, y32)
     torch.cuda.synchronize()
     r = torch.view_as_real(y32).half().float().cpu().numpy()
+    # one FP16 ulp, plus the FP32 paths' own rounding differences (absolute, at the
+    # transform's scale), which can move a value near zero by more than its ulp
     ulp = np.abs(np.spacing(r.astype(np.float16)).astype(np.float64))
-    assert np.all(np.abs(y - r) <= ulp + 1e-30)
+    assert np.all(np.abs(y - r) <= ulp + 1e-6 * np.log2(n) * np.abs(r).max())
     # in place
     assert fft.asdFftExecC2C(plan.handle, a, a) == fft.ACL_SUCCESS
     torch.cuda.synchronize()

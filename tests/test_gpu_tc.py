@@ -129,6 +129,29 @@ def test_real_transforms(cuda, n, direction, precision):
 
 
 @pytest.mark.parametrize("precision", MODES, ids=["fp16x3", "bf16x3"])
+@pytest.mark.parametrize("direction", [FWD, INV], ids=["fwd", "inv"])
+def test_256_point_stage(cuda, direction, precision):
+    """The 16 x 16 tensor-core DFT stage: rows, columns of a 3D volume, and the
+    packed half of a 512-point real transform."""
+    rng = np.random.default_rng(256 + direction)
+    f = direction == FWD
+    x = _rand_complex(rng, (8 * 37 + 3, 256))
+    y, desc = _run([256], C2C, direction, x.shape[0], x, precision)
+    assert "tensor-core" in desc, desc
+    assert oracle.rel_l2(y, oracle.c2c(x, f)) <= oracle.tolerance(256)
+    model = tc_model.tc_fft(x[:16], f, 0 if precision == fft.PRECISION_FP16X3 else 1)
+    assert oracle.rel_l2(y[:16], model) <= 2e-6 if precision == fft.PRECISION_FP16X3 else True
+    v = _rand_complex(rng, (2, 32, 256, 256))
+    y, desc = _run([32, 256, 256], C2C, direction, 2, v, precision)
+    assert desc.count("tensor-core") == 2, desc  # the 256-point Y and Z axes (X = 32 stays FP32)
+    assert oracle.rel_l2(y, oracle.c2c(v, f, ndim=3)) <= oracle.tolerance(32 * 256 * 256)
+    xr = rng.standard_normal((17, 512)).astype(np.float32)
+    y, desc = _run([512], R2C, direction, 17, xr, precision)
+    assert "tensor-core" in desc, desc
+    assert oracle.rel_l2(y, oracle.r2c(xr, f)) <= oracle.tolerance(512)
+
+
+@pytest.mark.parametrize("precision", MODES, ids=["fp16x3", "bf16x3"])
 def test_2d_2048(cuda, precision):
     rng = np.random.default_rng(8)
     x = _rand_complex(rng, (2, 2048, 2048))
