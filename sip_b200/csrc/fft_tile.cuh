@@ -116,6 +116,10 @@ struct TileDesc {
     // the input, bit 1 = the output.  Loads widen to FP32, the stages run in
     // FP32, stores round to FP16 (round to nearest even).
     int half_io;
+    // Shared-memory float2 count of one tile buffer of the TMA column kernel
+    // (col_pipe.cu): >= tb * max(n, pitch), a multiple of 16 (128-byte aligned
+    // buffers).
+    int64_t col_buf;
 };
 
 // Stockham column of tile column c for the pass twiddle: (c / g_div) mod g_ns.

@@ -222,6 +222,7 @@ struct Builder {
             s.row_fn = nullptr;
             s.db = false;
             s.db_fn = nullptr;
+            s.cp_fn = nullptr;
             s.tc_fmt = -1;
             s.what += " [separated re/im]";
         }
@@ -314,6 +315,19 @@ struct Builder {
                     s.db_stw = stw;
                 }
                 s.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(d.num_tiles, int64_t(per_sm) * sm_count(device))));
+            }
+            // TMA column tiles of the same engine: box copies instead of per-element
+            // copies, last stage stored from registers
+            const void *cfn = s.db_fn ? col_pipe_kernel_fn(n, d.tpt, d.tb, s.forward) : nullptr;
+            if (cfn && col_pipe_layout_ok(d)) {
+                const int64_t need = int64_t(d.tb) * std::max(n, d.pitch);
+                d.col_buf = (need + 15) / 16 * 16;
+                const int cps = kernel_blocks_per_sm(cfn, d.tb * d.tpt, col_pipe_smem(d));
+                if (cps > 0) {
+                    s.cp_fn = cfn;
+                    s.cp_grid = static_cast<int>(
+                        std::max<int64_t>(1, std::min<int64_t>(d.num_tiles, int64_t(cps) * sm_count(device))));
+                }
             }
         }
         if (p.precision != 0 && p.fft_type != 0x30 && (io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
@@ -982,7 +996,9 @@ std::string describe_plan(const Plan &p)
     for (const Step &s : p.steps) {
         o << "  [" << static_cast<int>(s.src) << "->" << static_cast<int>(s.dst) << "] " << s.what;
         if (s.kind == StepKind::kTile) {
-            o << (s.db ? (s.db_fn ? " [double-buffered, static engine]" : " [double-buffered]") : "") << " n=" << s.d.n
+            o << (s.cp_fn ? " [TMA column tiles, static engine]"
+                          : (s.db ? (s.db_fn ? " [double-buffered, static engine]" : " [double-buffered]") : ""))
+              << " n=" << s.d.n
               << " radices=";
             for (int i = 0; i < s.d.nstages; i++) o << (i ? "x" : "") << s.d.radix[i];
             o << " tb=" << s.d.tb << " tpt=" << s.d.tpt << " tiles=" << s.d.num_tiles << " grid=" << s.grid

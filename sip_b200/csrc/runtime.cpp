@@ -159,6 +159,7 @@ cudaError_t configure_kernels(int device)
     static_kernel_fns(fns);
     tc_kernel_fns(fns);
     tc_rows_kernel_fns(fns);
+    col_pipe_kernel_fns(fns);
     for (const void *fn : fns) {
         cudaError_t e = allow_max_dynamic_smem(fn);
         if (e != cudaSuccess) return e;
@@ -204,6 +205,7 @@ std::string complex32_steps(const Plan &p, std::vector<Step> &out)
         s->row_fn = nullptr;
         s->db = false;
         s->db_fn = nullptr;
+        s->cp_fn = nullptr;
     }
     out.front().d.half_io |= 1;
     out.back().d.half_io |= 2;
@@ -285,6 +287,12 @@ cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const v
                                              st);
                     else
                         e = launch_row_tiles(d, s.maxe, s.forward, s.row_grid, device_error_word(p.device), st);
+                } else if (s.cp_fn && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+                    TileDesc d = s.d;
+                    d.in = src;
+                    d.out = dst;
+                    d.stw = s.db_stw;
+                    e = launch_col_pipe(s.cp_fn, d, s.cp_grid, device_error_word(p.device), st);
                 } else if (s.db) {
                     TileDesc d = s.d;
                     d.in = src;

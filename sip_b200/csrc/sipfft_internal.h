@@ -65,6 +65,15 @@ struct StaticKernel {
     int row_bufs = 2;           // shared-memory buffers of its row kernel (3: ping-pong work area)
 };
 const StaticKernel *find_static_kernel(int n, int io);
+// TMA-pipelined column kernels (col_pipe.cu) for the power-of-two static
+// engines with 16 points per thread: n, threads per transform and columns per
+// tile must match an instantiation.
+const void *col_pipe_kernel_fn(int n, int tpt, int tb, bool forward);
+void col_pipe_kernel_fns(std::vector<const void *> &out);
+size_t col_pipe_smem(const TileDesc &d);
+// the step's input addressing and sizes fit the tensor map of the column kernel
+bool col_pipe_layout_ok(const TileDesc &d);
+cudaError_t launch_col_pipe(const void *fn, const TileDesc &d, int grid, int *err, cudaStream_t st);
 cudaError_t fill_stage_twiddles(float2 *t, const int *radix, int nstages, cudaStream_t st);
 int64_t stage_twiddle_count(const int *radix, int nstages);
 // Tensor-core split-precision stages (tc_fft.cu): n = n1 * n2 as two DFT-matrix
@@ -165,6 +174,9 @@ struct Step {
     bool db = false;  // run d on the double-buffered tile kernel (grid is then persistent)
     const void *db_fn = nullptr;  // compile-time engine for it (else the runtime-radix kernel)
     const float2 *db_stw = nullptr;  // that engine's per-stage twiddle tables
+    // TMA column kernel of the same engine (used when the source is 16-byte aligned)
+    const void *cp_fn = nullptr;
+    int cp_grid = 1;
     bool has_row = false;
     TileDesc rd{};
     int row_grid = 1;

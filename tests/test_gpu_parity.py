@@ -363,3 +363,29 @@ def test_complex32_refused_where_unsupported(cuda):
     assert fft.asdFftExecC2C(plan.handle, a, a) == fft.ACL_ERROR_API_NOT_SUPPORT
     a.close()
     plan.close()
+
+
+@pytest.mark.parametrize("n,batch", [(256, 64), (2048, 20), (65536, 6), (1024, 10)])
+def test_tma_column_tiles_and_fallback_agree(cuda, n, batch):
+    """A 16-byte aligned source of a strided axis takes the TMA column-tile
+    kernel; an 8-byte aligned one the double-buffered element-copy kernel.
+    Both give the oracle's result (vertical 1D; 65536 runs as two passes)."""
+    import torch
+
+    rng = np.random.default_rng(n + batch)
+    x = _rand_complex(rng, (n, batch))
+    plan = fft.FftPlan([n], C2C, FWD, batch, fft.ASCEND_FFT_VERTICAL)
+    assert "TMA column tiles" in plan.describe(), plan.describe()
+    ref = oracle.c2c(x.T, True).T
+    outs = []
+    for shift in (0, 1):
+        flat = torch.zeros(x.size + 4, dtype=torch.complex64, device="cuda")
+        flat[shift:shift + x.size] = torch.from_numpy(x.reshape(-1)).cuda()
+        out = torch.empty((n, batch), dtype=torch.complex64, device="cuda")
+        assert plan.exec_raw(flat.data_ptr() + 8 * shift, out.data_ptr()) == fft.ACL_SUCCESS
+        torch.cuda.synchronize()
+        assert fft.asdFftSynchronize(plan.handle) == fft.ACL_SUCCESS
+        outs.append(out.cpu().numpy())
+        assert oracle.rel_l2(outs[-1], ref) <= oracle.tolerance(n), shift
+    assert np.max(np.abs(outs[0] - outs[1])) <= 1e-5 * np.max(np.abs(ref))
+    plan.close()
