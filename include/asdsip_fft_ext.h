@@ -33,6 +33,8 @@ ASDSIP_API int32_t asdFftPlanLaunchCount(void *handle);
  * mode 1: tensor-core (tcgen05) DFT-matrix stages, operands split into FP16 hi + lo parts with a
  *         power-of-two scale per tile, three products hi*hi + hi*lo + lo*hi accumulated in FP32.
  * mode 2: the same with BF16 hi + lo parts (no scaling; about 16 significant bits per operand).
+ * mode 3: per transform length, the arithmetic that the autotuner (asdFftAutotune, or a cache loaded
+ *         with asdFftTuneCacheLoad) measured fastest on this GPU; FP32 for lengths it has not timed.
  * Tensor-core stages exist for transform lengths 256, 1024, 2048 and 4096 of a C2C axis (and 512, 2048,
  * 4096 and 8192 for R2C / C2R, whose packed inner transform has half the length); every other step keeps the FP32
  * kernels, which asdFftDescribePlan shows.  May be called before or after MakePlan*: an initialised
@@ -53,9 +55,12 @@ ASDSIP_API int32_t asdFftBatchExec(void *plan, const void *input, void *output, 
 ASDSIP_API int32_t asdFftBatchPlanDestroy(void *plan);
 ASDSIP_API int64_t asdFftBatchDescribe(void *plan, char *buf, int64_t len);
 
-/* ---- autotuner: times radix orders and elements per thread for each length (rows[i] transforms, capped at 256)
- * and keeps the fastest per length; cache_path (optional) receives one JSON object per line keyed by
- * GPU name, type, precision and length.  TuneCacheLoad returns the number of entries loaded for this GPU. */
+/* ---- autotuner: for each length (rows[i] transforms, capped at 256) times the radix orders, elements per
+ * thread and tile shapes (threads per CTA) of the SIMT tile kernels and keeps the fastest (uneven-batch
+ * plans use it), and for lengths with a tensor-core stage times the whole plan in FP32 and in the FP16 x3
+ * and BF16 x3 forms and keeps the fastest (plans in precision mode 3 use it).  cache_path (optional)
+ * receives one JSON object per line keyed by GPU name, type and length.  TuneCacheLoad returns the number
+ * of entries loaded for this GPU. */
 ASDSIP_API int32_t asdFftAutotune(const int64_t *sizes, const int64_t *rows, int32_t n, int32_t direction,
                                   const char *cache_path);
 ASDSIP_API int32_t asdFftTuneCacheLoad(const char *cache_path);

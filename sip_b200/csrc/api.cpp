@@ -658,7 +658,7 @@ int64_t asdFftGetErrorMessage(char *buf, int64_t len)
 int32_t asdFftSetPrecision(void *handle, int32_t mode)
 {
     sipfft::Plan *p = find_plan(handle);
-    if (!p || mode < 0 || mode > 2) {
+    if (!p || mode < 0 || mode > 3) {
         log_error("asdFftSetPrecision", "unknown handle or precision mode");
         return AsdSip::ACL_ERROR_INVALID_PARAM;
     }

@@ -1,5 +1,7 @@
 // Uneven batches in one persistent launch, captured in a CUDA graph, and the
-// autotuner that picks the radix order and elements per thread per length.
+// autotuner that picks, per length, the radix order, elements per thread and
+// tile shape of the SIMT tile kernels, and the stage arithmetic (FP32 SIMT or
+// a split-precision tensor-core form) of ordinary plans in precision mode 3.
 //
 // An uneven batch is a list of groups (length n_i, count b_i) of 1D C2C
 // transforms stored back to back.  Every group is planned with the ordinary
@@ -64,7 +66,10 @@ std::string gpu_name(int device)
 }
 
 // Cache file: one JSON object per line,
-// {"gpu": "...", "type": "c2c", "precision": "fp32", "n": 4096, "radices": [16,16,16], "maxe": 16, "us": 12.5}
+// {"gpu": "...", "type": "c2c", "precision": "fp32", "n": 4096, "radices": [16,16,16], "maxe": 16,
+//  "row_threads": 256, "us": 12.5, "plan_us": 30.1}
+// radices / maxe / row_threads: the SIMT tile kernels' choice (us: its time);
+// precision: the arithmetic that ran the whole plan fastest (plan_us).
 bool parse_line(const std::string &line, std::string &gpu, int64_t &n, TuneChoice &c)
 {
     auto field = [&](const char *key) -> std::string {
@@ -95,7 +100,11 @@ bool parse_line(const std::string &line, std::string &gpu, int64_t &n, TuneChoic
     while (std::getline(ss, tok, ',')) c.radices.push_back(std::atoi(tok.c_str()));
     c.maxe = std::atoi(ms.c_str());
     c.us = std::atof(us.c_str());
-    return n > 0 && valid_radices(c.radices, n);
+    c.row_threads = std::atoi(field("row_threads").c_str());
+    const std::string pr = field("precision");
+    c.precision = pr == "fp16x3" ? 1 : (pr == "bf16x3" ? 2 : 0);
+    c.plan_us = std::atof(field("plan_us").c_str());
+    return n > 0 && valid_radices(c.radices, n) && c.row_threads >= 0 && c.row_threads <= 512;
 }
 
 }  // namespace
@@ -137,10 +146,13 @@ bool save_tune_cache(const std::string &path, int device)
     for (const auto &l : keep) o << l << "\n";
     std::lock_guard<std::mutex> lock(g_tune_mu);
     for (const auto &kv : g_tuned) {
-        o << "{\"gpu\": \"" << me << "\", \"type\": \"c2c\", \"precision\": \"fp32\", \"n\": " << kv.first
-          << ", \"radices\": [";
-        for (size_t i = 0; i < kv.second.radices.size(); i++) o << (i ? "," : "") << kv.second.radices[i];
-        o << "], \"maxe\": " << kv.second.maxe << ", \"us\": " << kv.second.us << "}\n";
+        static const char *kForm[] = {"fp32", "fp16x3", "bf16x3"};
+        const TuneChoice &c = kv.second;
+        o << "{\"gpu\": \"" << me << "\", \"type\": \"c2c\", \"precision\": \"" << kForm[c.precision % 3]
+          << "\", \"n\": " << kv.first << ", \"radices\": [";
+        for (size_t i = 0; i < c.radices.size(); i++) o << (i ? "," : "") << c.radices[i];
+        o << "], \"maxe\": " << c.maxe << ", \"row_threads\": " << c.row_threads << ", \"us\": " << c.us
+          << ", \"plan_us\": " << c.plan_us << "}\n";
     }
     return static_cast<bool>(o);
 }
@@ -187,11 +199,17 @@ std::vector<TuneChoice> tune_candidates(int64_t n)
     orders.erase(std::unique(orders.begin(), orders.end()), orders.end());
     for (const auto &o : orders) {
         for (int maxe : {8, 16, 32}) {
-            if ((n + maxe - 1) / maxe > 512) continue;
-            TuneChoice c;
-            c.radices = o;
-            c.maxe = maxe;
-            out.push_back(c);
+            const int tpt = static_cast<int>((n + maxe - 1) / maxe);
+            if (tpt > 512) continue;
+            // tile shape: transforms per CTA so that a CTA has about this many threads
+            for (int threads : {64, 128, 256}) {
+                if (threads < tpt && threads != 256) continue;
+                TuneChoice c;
+                c.radices = o;
+                c.maxe = maxe;
+                c.row_threads = threads;
+                out.push_back(c);
+            }
         }
     }
     return out;
@@ -250,6 +268,39 @@ int autotune_lengths(const std::vector<int64_t> &sizes, const std::vector<int64_
             cudaEventElapsedTime(&ms, e0, e1);
             c.us = ms * 1e3 / 5.0;
             if (c.us < best.us) best = c;
+        }
+        // whole-plan arithmetic per length (ordinary plans in precision mode 3):
+        // the FP32 kernels against the split-precision tensor-core forms
+        TcConfig tcc;
+        if (best.us < 1e29 && (tc_config(static_cast<int>(n), tcc) || tc_rows_config(static_cast<int>(n), tcc))) {
+            best.plan_us = 1e30;
+            for (int form = 0; form < 3; form++) {
+                Plan q;
+                q.fft_type = 0x10;
+                q.direction = forward ? 0x10 : 0x11;
+                q.sizes = {n};
+                q.batch = rows_per[i];
+                q.device = device;
+                q.precision = form;
+                if (!build_plan_1d(q).empty() || q.ws_bytes > 0) continue;
+                bool ok = true;
+                for (int rep = 0; rep < 2 && ok; rep++) ok = execute_plan(q, buf, out, 0) == cudaSuccess;
+                cudaEventRecord(e0, 0);
+                for (int rep = 0; rep < 5 && ok; rep++) ok = execute_plan(q, buf, out, 0) == cudaSuccess;
+                cudaEventRecord(e1, 0);
+                if (!ok || cudaEventSynchronize(e1) != cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                const double us = ms * 1e3 / 5.0;
+                if (us < best.plan_us) {
+                    best.plan_us = us;
+                    best.precision = form;
+                }
+            }
+            if (best.plan_us >= 1e29) best.plan_us = 0.0;
         }
         if (best.us < 1e29) {
             set_tuned_choice(n, best);

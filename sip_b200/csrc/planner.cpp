@@ -249,13 +249,15 @@ struct Builder {
             return false;
         }
         int maxe_override = 0;
+        int row_threads = p.row_threads;
         TuneChoice tc;
         if (p.use_tuned && tuned_choice(n, tc) && valid_radices(tc.radices, n) && tc.maxe <= p.max_maxe) {
             radices = tc.radices;
             maxe_override = tc.maxe;
+            if (tc.row_threads > 0 && tc.row_threads <= p.row_threads) row_threads = tc.row_threads;
         }
         TileCfg c;
-        if (!choose_cfg(n, column, n_cols, c, err, maxe_override, p.row_threads, p.row_smem, p.max_maxe,
+        if (!choose_cfg(n, column, n_cols, c, err, maxe_override, row_threads, p.row_smem, p.max_maxe,
                         p.max_maxe < 32 ? p.row_threads : kMaxThreads))
             return false;
         s = Step();
@@ -330,18 +332,23 @@ struct Builder {
                 }
             }
         }
-        if (p.precision != 0 && p.fft_type != 0x30 && (io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
-            return add_tc_variant(s);
-        return true;
+        if (p.fft_type == 0x30 || !(io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED)) return true;
+        int form = p.precision;
+        if (form == 3) {
+            // per length, the arithmetic the autotuner measured fastest
+            TuneChoice t;
+            form = tuned_choice(n, t) ? t.precision : 0;
+        }
+        return form == 1 || form == 2 ? add_tc_variant(s, form) : true;
     }
 
     // Tensor-core split-precision form of a tile step (lengths with a
     // tcgen05 kernel); replaces the FP32 kernels of the step.
-    bool add_tc_variant(Step &s)
+    bool add_tc_variant(Step &s, int form)
     {
         TcConfig tc;
         const int n = s.d.n;
-        const int fmt_rows = p.precision == 1 ? 0 : 1;
+        const int fmt_rows = form == 1 ? 0 : 1;
         if (s.d.io == IO_C2C && !s.d.xfast && s.d.n_outer == 1 && s.d.in_a.estride == 1 && s.d.out_a.estride == 1 &&
             tc_rows_config(n, tc)) {
             // contiguous C2C rows: the warp-specialised row pipeline
@@ -371,7 +378,7 @@ struct Builder {
             }
         }
         if (!tc_config(n, tc)) return true;
-        const int fmt = p.precision == 1 ? 0 : 1;
+        const int fmt = form == 1 ? 0 : 1;
         size_t smem = 0;
         const void *fn = tc_kernel(n, fmt, s.forward, &smem);
         if (!fn) return true;

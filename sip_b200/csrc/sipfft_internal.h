@@ -193,11 +193,17 @@ struct Step {
     std::string what;  // human-readable description (plan dump)
 };
 
-// Autotuned choice for one length: radix order and elements per thread.
+// Autotuned choice for one length: radix order, elements per thread and
+// tile shape (threads per CTA that the tile kernels aim for, 0 = planner
+// default) of the SIMT tile kernels, and the stage arithmetic that ran the
+// whole plan fastest (0 FP32 SIMT, 1 tensor-core FP16 x3, 2 BF16 x3).
 struct TuneChoice {
     std::vector<int> radices;
     int maxe = 0;
+    int row_threads = 0;
     double us = 0.0;
+    int precision = 0;
+    double plan_us = 0.0;  // time of the whole plan in the chosen arithmetic
 };
 
 struct Plan {
@@ -229,7 +235,8 @@ struct Plan {
     bool istft = false;
     int64_t istft_channel = 0, istft_frames = 0, istft_nfft = 0, istft_hop = 0, istft_out_len = 0;
     // 0: FP32 kernels; 1: tensor-core FP16 hi/lo x3; 2: tensor-core BF16 hi/lo x3
-    // (lengths without a tensor-core stage keep the FP32 kernels)
+    // (lengths without a tensor-core stage keep the FP32 kernels); 3: per length,
+    // the arithmetic the autotuner measured fastest (FP32 when untuned)
     int precision = 0;
     // complex32 (FP16 pairs) variant of a 1D C2C plan's steps, built at the
     // first complex32 exec (c32_state: 0 not built, 1 built, -1 unsupported)

@@ -48,6 +48,7 @@ ASCEND_FFT_VERTICAL = 0x11
 PRECISION_FP32 = 0       # CUDA-core FP32 kernels
 PRECISION_FP16X3 = 1     # tensor-core DFT-matrix stages, FP16 hi/lo split, 3 products, FP32 accumulate
 PRECISION_BF16X3 = 2     # the same with BF16 hi/lo parts
+PRECISION_AUTO = 3       # per length, the arithmetic the autotuner measured fastest
 
 ACL_FLOAT = 0
 ACL_COMPLEX64 = 16

@@ -74,10 +74,10 @@ def test_plan_parameter_checks_before_device(lib):
         assert lib.asdFftExecRaw(h, ctypes.c_void_p(8), ctypes.c_void_p(16)) == fft.ACL_ERROR_INVALID_PARAM
         st, typ = fft.asdFftGetType(h)
         assert st == fft.ACL_SUCCESS
-        # precision modes 0..2; anything else (or an unknown handle) is a parameter error
-        for mode in (fft.PRECISION_FP16X3, fft.PRECISION_BF16X3, fft.PRECISION_FP32):
+        # precision modes 0..3; anything else (or an unknown handle) is a parameter error
+        for mode in (fft.PRECISION_FP16X3, fft.PRECISION_BF16X3, fft.PRECISION_AUTO, fft.PRECISION_FP32):
             assert lib.asdFftSetPrecision(h, mode) == fft.ACL_SUCCESS
-        assert lib.asdFftSetPrecision(h, 3) == fft.ACL_ERROR_INVALID_PARAM
+        assert lib.asdFftSetPrecision(h, 4) == fft.ACL_ERROR_INVALID_PARAM
         assert lib.asdFftSetPrecision(h, -1) == fft.ACL_ERROR_INVALID_PARAM
         assert lib.asdFftSetPrecision(ctypes.c_void_p(0x1234), 1) == fft.ACL_ERROR_INVALID_PARAM
     finally:

@@ -64,9 +64,38 @@ def test_autotune_cache_round_trip(cuda, tmp_path):
     lines = [json.loads(l) for l in open(path)]
     assert {l["n"] for l in lines} >= {1500, 2048, 105}
     for l in lines:
-        assert l["type"] == "c2c" and l["precision"] == "fp32" and l["gpu"]
+        assert l["type"] == "c2c" and l["precision"] in ("fp32", "fp16x3", "bf16x3") and l["gpu"]
         assert int(np.prod(l["radices"])) == l["n"]
+        assert l["row_threads"] in (64, 128, 256)
+    # 2048 has tensor-core stages: the whole plan was timed in every arithmetic
+    assert [l for l in lines if l["n"] == 2048][0]["plan_us"] > 0
     assert fft.tune_cache_load(path) >= 3
     plan, x, outs = _run(groups, fft.ASCEND_FFT_FORWARD, tune_cache=path)
     _check(plan, x, outs[0], True)
     plan.close()
+
+
+def test_precision_auto_follows_the_tuned_arithmetic(cuda, tmp_path):
+    """Precision mode 3: each length runs in the arithmetic its cache entry
+    names (here a tensor-core form for 2048 and FP32 for 1024), with parity."""
+    import torch
+
+    path = str(tmp_path / "tune.jsonl")
+    gpu = torch.cuda.get_device_name(0)
+    with open(path, "w") as f:
+        f.write(json.dumps({"gpu": gpu, "type": "c2c", "precision": "fp16x3", "n": 2048, "radices": [16, 16, 8],
+                            "maxe": 16, "row_threads": 256, "us": 1.0, "plan_us": 1.0}) + "\n")
+        f.write(json.dumps({"gpu": gpu, "type": "c2c", "precision": "fp32", "n": 1024, "radices": [16, 16, 4],
+                            "maxe": 16, "row_threads": 256, "us": 1.0, "plan_us": 1.0}) + "\n")
+    assert fft.tune_cache_load(path) == 2
+    rng = np.random.default_rng(9)
+    for n, want_tc in ((2048, True), (1024, False)):
+        x = (rng.uniform(-1, 1, (24, n)) + 1j * rng.uniform(-1, 1, (24, n))).astype(np.complex64)
+        plan = fft.FftPlan([n], fft.ASCEND_FFT_C2C, fft.ASCEND_FFT_FORWARD, 24, precision=fft.PRECISION_AUTO)
+        assert ("tensor-core" in plan.describe()) == want_tc, plan.describe()
+        xd = torch.from_numpy(x).cuda()
+        y = torch.empty_like(xd)
+        plan(xd, y)
+        torch.cuda.synchronize()
+        assert oracle.rel_l2(y.cpu().numpy(), oracle.c2c(x, True)) <= oracle.tolerance(n)
+        plan.close()
