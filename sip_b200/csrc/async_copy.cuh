@@ -85,6 +85,18 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
+// Programmatic dependent launch.  An FFT kernel launched with programmatic
+// stream serialization may become resident while the previous kernel on its
+// stream is still draining its last tiles; it waits here until that kernel
+// has completed and its memory is visible, before its first global access,
+// and then allows the next kernel on the stream to launch the same way.
+// Launched without the attribute, both instructions do nothing.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Output element store that allocates no L1 line: streamed FFT output would
 // otherwise evict the twiddle tables that the next tiles read from L1.
 __device__ __forceinline__ void st_stream(float2 *p, float2 v)

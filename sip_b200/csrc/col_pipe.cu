@@ -64,6 +64,7 @@ template <class Q, int T, int TB, bool FWD>
 __global__ void __launch_bounds__(TB *T, (TB * T <= 256) ? 2 : 1)
     col_pipe_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ TileDesc d, int *err)
 {
+    pdl_enter();
     using E = StaticEngine<Q, T>;
     constexpr int N = Q::N;
     constexpr int BOX = N < 256 ? N : 256;
@@ -215,7 +216,7 @@ cudaError_t launch_col_pipe(const void *fn, const TileDesc &d, int grid, int *er
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
     TileDesc dd = d;
     void *args[] = {&map, &dd, &err};
-    return cudaLaunchKernel(fn, dim3(grid), dim3(d.tb * d.tpt), args, col_pipe_smem(d), st);
+    return launch_pdl(fn, dim3(grid), dim3(d.tb * d.tpt), col_pipe_smem(d), st, args);
 }
 
 }  // namespace sipfft

@@ -184,6 +184,7 @@ __device__ __forceinline__ void process_tile(const TileDesc &d, const void *in, 
 template <int MAXE, bool FWD>
 __global__ void __launch_bounds__(512, 1) tile_fft_kernel(const __grid_constant__ TileDesc d)
 {
+    pdl_enter();
     extern __shared__ float2 sm[];
     for (int64_t g = blockIdx.x; g < d.num_tiles; g += gridDim.x) process_tile<MAXE, FWD>(d, d.in, d.out, g, sm);
 }
@@ -196,6 +197,7 @@ __global__ void __launch_bounds__(512, 1) tile_fft_kernel(const __grid_constant_
 template <int MAXE, bool FWD>
 __global__ void __launch_bounds__(512, 1) tile_db_kernel(const __grid_constant__ TileDesc d)
 {
+    pdl_enter();
     extern __shared__ float2 sm[];
     const int64_t span = int64_t(d.tb) * d.pitch;
     const int tid = threadIdx.x;
@@ -416,8 +418,10 @@ namespace {
 template <int MAXE, bool FWD>
 cudaError_t launch_one(const TileDesc &d, int grid, int block, size_t smem, cudaStream_t st)
 {
-    tile_fft_kernel<MAXE, FWD><<<grid, block, smem, st>>>(d);
-    return cudaGetLastError();
+    TileDesc dd = d;
+    void *args[] = {&dd};
+    return launch_pdl(reinterpret_cast<const void *>(tile_fft_kernel<MAXE, FWD>), dim3(grid), dim3(block), smem, st,
+                      args);
 }
 }  // namespace
 
@@ -455,7 +459,7 @@ cudaError_t launch_tile_db(const TileDesc &d, int maxe, bool forward, int grid, 
         return cudaErrorInvalidConfiguration;
     TileDesc dd = d;
     void *args[] = {&dd};
-    return cudaLaunchKernel(tile_db_kernel_fn(maxe, forward), dim3(grid), dim3(block), args, smem, st);
+    return launch_pdl(tile_db_kernel_fn(maxe, forward), dim3(grid), dim3(block), smem, st, args);
 }
 
 cudaError_t launch_tile(const TileDesc &d, int maxe, bool forward, int grid, cudaStream_t st)

@@ -132,6 +132,7 @@ template <class Engine, bool FWD, int IO>
 __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
     pipelined_rows_kernel(const __grid_constant__ TileDesc d, int *err)
 {
+    pdl_enter();
     extern __shared__ __align__(128) unsigned char smraw[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smraw);
     const int64_t buf_f2 = d.g_ns;  // per-buffer float2 count (planner-computed, even)

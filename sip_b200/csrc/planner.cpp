@@ -159,6 +159,7 @@ struct Builder {
     explicit Builder(Plan &plan) : p(plan), fwd(plan.forward()), device(plan.device) {}
 
     std::string err;
+    bool in_multipass = false;  // planning the passes of a multi-pass transform
 
     const float2 *table(int64_t count, int64_t denom, int64_t mult = 1)
     {
@@ -332,7 +333,10 @@ struct Builder {
                 }
             }
         }
-        if (p.fft_type == 0x30 || !(io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED)) return true;
+        // passes of a multi-pass transform keep the FP32 kernels: their tiles would run on the
+        // single-tile tensor-core kernel, several times slower than the double-buffered FP32 passes
+        if (in_multipass || p.fft_type == 0x30 || !(io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
+            return true;
         int form = p.precision;
         if (form == 3) {
             // per length, the arithmetic the autotuner measured fastest
@@ -504,6 +508,11 @@ struct Builder {
         Buf cur = src;
         int64_t cur_dist = in_dist;
         int64_t ns = 1;
+        struct Flag {
+            bool &f;
+            explicit Flag(bool &x) : f(x) { f = true; }
+            ~Flag() { f = false; }
+        } flag(in_multipass);
         for (size_t i = 0; i < passes.size(); i++) {
             const int rp = passes[i];
             const bool last = i + 1 == passes.size();

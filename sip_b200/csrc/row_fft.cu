@@ -59,13 +59,28 @@ int kernel_blocks_per_sm(const void *fn, int threads, size_t smem)
     return nb;
 }
 
+cudaError_t launch_pdl(const void *fn, dim3 grid, dim3 block, size_t smem, cudaStream_t st, void **args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
 cudaError_t launch_kernel_fn(const void *fn, const TileDesc &d, int grid, size_t smem, int *err, cudaStream_t st)
 {
     if (!fn || d.tb * d.tpt > 512 || smem > static_cast<size_t>(kMaxSmemBytes) || grid <= 0)
         return cudaErrorInvalidConfiguration;
     TileDesc dd = d;
     void *args[] = {&dd, &err};
-    return cudaLaunchKernel(fn, dim3(grid), dim3(d.tb * d.tpt), args, smem, st);
+    return launch_pdl(fn, dim3(grid), dim3(d.tb * d.tpt), smem, st, args);
 }
 
 void row_kernel_fns(std::vector<const void *> &out)

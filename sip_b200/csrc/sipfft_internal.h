@@ -52,6 +52,9 @@ const void *batch_kernel_fn(bool forward);
 cudaError_t launch_batch(int grid, int block, size_t smem, const BatchSeg *segs, const int2 *items, int nitems,
                          int *counter, int *done, const BatchBufs &bufs, int *err, bool forward, cudaStream_t st);
 cudaError_t launch_kernel_fn(const void *fn, const TileDesc &d, int grid, size_t smem, int *err, cudaStream_t st);
+// Launch with programmatic stream serialization (the kernel calls pdl_enter()
+// before its first global access).
+cudaError_t launch_pdl(const void *fn, dim3 grid, dim3 block, size_t smem, cudaStream_t st, void **args);
 
 // Compile-time specialised pipelined row kernels (static_fft.cu).
 struct StaticKernel {

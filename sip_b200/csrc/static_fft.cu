@@ -28,6 +28,7 @@ struct PassRow {
 template <class E, bool FWD>
 __global__ void __launch_bounds__(512, 1) static_db_kernel(const __grid_constant__ TileDesc d, int *)
 {
+    pdl_enter();
     extern __shared__ float2 sm[];
     const int64_t span = int64_t(d.tb) * d.pitch;
     const int tid = threadIdx.x;
