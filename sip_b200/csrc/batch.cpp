@@ -198,12 +198,13 @@ std::vector<TuneChoice> tune_candidates(int64_t n)
     std::sort(orders.begin(), orders.end());
     orders.erase(std::unique(orders.begin(), orders.end()), orders.end());
     for (const auto &o : orders) {
-        for (int maxe : {8, 16, 32}) {
+        for (int maxe : {8, 16}) {
             const int tpt = static_cast<int>((n + maxe - 1) / maxe);
-            if (tpt > 512) continue;
-            // tile shape: transforms per CTA so that a CTA has about this many threads
-            for (int threads : {64, 128, 256}) {
-                if (threads < tpt && threads != 256) continue;
+            if (tpt > kBatchBlock) continue;
+            // tile shape: transforms per tile so that a tile has about this many threads
+            // (the batch kernel's CTA has 256)
+            for (int threads : {128, 256}) {
+                if (threads < tpt) continue;
                 TuneChoice c;
                 c.radices = o;
                 c.maxe = maxe;
@@ -213,105 +214,6 @@ std::vector<TuneChoice> tune_candidates(int64_t n)
         }
     }
     return out;
-}
-
-// Times each candidate as a stand-alone tile launch over `rows` transforms
-// and records the fastest.  Returns the number of lengths tuned.
-int autotune_lengths(const std::vector<int64_t> &sizes, const std::vector<int64_t> &rows_per, bool forward,
-                     int device, std::string *err)
-{
-    int tuned = 0;
-    int64_t max_elems = 0;
-    for (size_t i = 0; i < sizes.size(); i++) max_elems = std::max(max_elems, sizes[i] * rows_per[i]);
-    if (max_elems == 0) return 0;
-    float2 *buf = nullptr, *out = nullptr;
-    if (cudaMalloc(&buf, max_elems * sizeof(float2)) != cudaSuccess ||
-        cudaMalloc(&out, max_elems * sizeof(float2)) != cudaSuccess) {
-        if (err) *err = "autotune: out of device memory";
-        cudaGetLastError();
-        cudaFree(buf);
-        return 0;
-    }
-    cudaMemset(buf, 0, max_elems * sizeof(float2));
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    for (size_t i = 0; i < sizes.size(); i++) {
-        const int64_t n = sizes[i];
-        if (n > 16384) continue;  // multi-pass lengths keep the planner's split
-        TuneChoice best;
-        best.us = 1e30;
-        for (TuneChoice c : tune_candidates(n)) {
-            set_tuned_choice(n, c);
-            Plan p;
-            p.fft_type = 0x10;
-            p.direction = forward ? 0x10 : 0x11;
-            p.sizes = {n};
-            p.batch = rows_per[i];
-            p.device = device;
-            p.use_tuned = true;
-            if (!build_plan_1d(p).empty() || p.steps.size() != 1) continue;
-            // the uneven-batch kernel runs the generic tile path: time that path
-            Step s = p.steps[0];
-            s.has_row = false;
-            p.steps[0] = s;
-            bool ok = true;
-            for (int rep = 0; rep < 2 && ok; rep++) ok = execute_plan(p, buf, out, 0) == cudaSuccess;
-            cudaEventRecord(e0, 0);
-            for (int rep = 0; rep < 5 && ok; rep++) ok = execute_plan(p, buf, out, 0) == cudaSuccess;
-            cudaEventRecord(e1, 0);
-            if (!ok || cudaEventSynchronize(e1) != cudaSuccess) {
-                cudaGetLastError();
-                continue;
-            }
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            c.us = ms * 1e3 / 5.0;
-            if (c.us < best.us) best = c;
-        }
-        // whole-plan arithmetic per length (ordinary plans in precision mode 3):
-        // the FP32 kernels against the split-precision tensor-core forms
-        TcConfig tcc;
-        if (best.us < 1e29 && (tc_config(static_cast<int>(n), tcc) || tc_rows_config(static_cast<int>(n), tcc))) {
-            best.plan_us = 1e30;
-            for (int form = 0; form < 3; form++) {
-                Plan q;
-                q.fft_type = 0x10;
-                q.direction = forward ? 0x10 : 0x11;
-                q.sizes = {n};
-                q.batch = rows_per[i];
-                q.device = device;
-                q.precision = form;
-                if (!build_plan_1d(q).empty() || q.ws_bytes > 0) continue;
-                bool ok = true;
-                for (int rep = 0; rep < 2 && ok; rep++) ok = execute_plan(q, buf, out, 0) == cudaSuccess;
-                cudaEventRecord(e0, 0);
-                for (int rep = 0; rep < 5 && ok; rep++) ok = execute_plan(q, buf, out, 0) == cudaSuccess;
-                cudaEventRecord(e1, 0);
-                if (!ok || cudaEventSynchronize(e1) != cudaSuccess) {
-                    cudaGetLastError();
-                    continue;
-                }
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                const double us = ms * 1e3 / 5.0;
-                if (us < best.plan_us) {
-                    best.plan_us = us;
-                    best.precision = form;
-                }
-            }
-            if (best.plan_us >= 1e29) best.plan_us = 0.0;
-        }
-        if (best.us < 1e29) {
-            set_tuned_choice(n, best);
-            tuned++;
-        }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaFree(buf);
-    cudaFree(out);
-    return tuned;
 }
 
 // ------------------------------------------------------------------------------------ batch plan
@@ -460,6 +362,115 @@ BatchPlan *find_batch(void *h)
 }
 
 }  // namespace
+
+// Times each candidate in the uneven-batch kernel (a one-group batch plan of
+// about 4 M points of the length) and records the fastest; for lengths with a
+// tensor-core stage also times the whole ordinary plan in each arithmetic.
+// Returns the number of lengths tuned.
+int autotune_lengths(const std::vector<int64_t> &sizes, const std::vector<int64_t> &rows_per, bool forward,
+                     int device, std::string *err)
+{
+    int tuned = 0;
+    int64_t max_elems = 0;
+    for (size_t i = 0; i < sizes.size(); i++)
+        max_elems = std::max(max_elems, std::max(sizes[i] * rows_per[i], int64_t(1) << 22) + sizes[i] * 16);
+    if (max_elems == 0) return 0;
+    float2 *buf = nullptr, *out = nullptr;
+    if (cudaMalloc(&buf, max_elems * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&out, max_elems * sizeof(float2)) != cudaSuccess) {
+        if (err) *err = "autotune: out of device memory";
+        cudaGetLastError();
+        cudaFree(buf);
+        return 0;
+    }
+    cudaMemset(buf, 0, max_elems * sizeof(float2));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (size_t i = 0; i < sizes.size(); i++) {
+        const int64_t n = sizes[i];
+        if (n > 16384) continue;  // multi-pass lengths keep the planner's split
+        TuneChoice best;
+        best.us = 1e30;
+        // enough transforms that a launch is not just its overhead
+        const int64_t rows = std::max<int64_t>(16, std::min<int64_t>((int64_t(1) << 22) / n, 4096));
+        for (TuneChoice c : tune_candidates(n)) {
+            set_tuned_choice(n, c);
+            // the uneven-batch kernel runs these tiles: time a one-group batch plan
+            BatchPlan bp;
+            bp.device = device;
+            bp.forward = forward;
+            bp.sizes = {n};
+            bp.batches = {rows};
+            if (!build_batch(bp).empty()) {
+                cudaGetLastError();
+                continue;
+            }
+            void *ws = nullptr;
+            if (bp.ws_bytes && cudaMalloc(&ws, bp.ws_bytes) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            bool ok = true;
+            for (int rep = 0; rep < 2 && ok; rep++) ok = enqueue(bp, buf, out, ws, 0) == cudaSuccess;
+            cudaEventRecord(e0, 0);
+            for (int rep = 0; rep < 5 && ok; rep++) ok = enqueue(bp, buf, out, ws, 0) == cudaSuccess;
+            cudaEventRecord(e1, 0);
+            ok = ok && cudaEventSynchronize(e1) == cudaSuccess;
+            if (ws) cudaFree(ws);
+            if (!ok) {
+                cudaGetLastError();
+                continue;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            c.us = ms * 1e3 / 5.0;
+            if (c.us < best.us) best = c;
+        }
+        // whole-plan arithmetic per length (ordinary plans in precision mode 3):
+        // the FP32 kernels against the split-precision tensor-core forms
+        TcConfig tcc;
+        if (best.us < 1e29 && (tc_config(static_cast<int>(n), tcc) || tc_rows_config(static_cast<int>(n), tcc))) {
+            best.plan_us = 1e30;
+            for (int form = 0; form < 3; form++) {
+                Plan q;
+                q.fft_type = 0x10;
+                q.direction = forward ? 0x10 : 0x11;
+                q.sizes = {n};
+                q.batch = rows;
+                q.device = device;
+                q.precision = form;
+                if (!build_plan_1d(q).empty() || q.ws_bytes > 0) continue;
+                bool ok = true;
+                for (int rep = 0; rep < 2 && ok; rep++) ok = execute_plan(q, buf, out, 0) == cudaSuccess;
+                cudaEventRecord(e0, 0);
+                for (int rep = 0; rep < 5 && ok; rep++) ok = execute_plan(q, buf, out, 0) == cudaSuccess;
+                cudaEventRecord(e1, 0);
+                if (!ok || cudaEventSynchronize(e1) != cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                const double us = ms * 1e3 / 5.0;
+                if (us < best.plan_us) {
+                    best.plan_us = us;
+                    best.precision = form;
+                }
+            }
+            if (best.plan_us >= 1e29) best.plan_us = 0.0;
+        }
+        if (best.us < 1e29) {
+            set_tuned_choice(n, best);
+            tuned++;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(buf);
+    cudaFree(out);
+    return tuned;
+}
 
 }  // namespace sipfft
 

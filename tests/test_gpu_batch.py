@@ -66,7 +66,7 @@ def test_autotune_cache_round_trip(cuda, tmp_path):
     for l in lines:
         assert l["type"] == "c2c" and l["precision"] in ("fp32", "fp16x3", "bf16x3") and l["gpu"]
         assert int(np.prod(l["radices"])) == l["n"]
-        assert l["row_threads"] in (64, 128, 256)
+        assert l["row_threads"] in (128, 256)
     # 2048 has tensor-core stages: the whole plan was timed in every arithmetic
     assert [l for l in lines if l["n"] == 2048][0]["plan_us"] > 0
     assert fft.tune_cache_load(path) >= 3
