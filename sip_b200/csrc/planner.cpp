@@ -107,6 +107,22 @@ bool choose_cfg(int n, bool column, int64_t ncols, TileCfg &c, std::string &err,
     return true;
 }
 
+// Resident CTAs per SM of the single-tile tensor-core kernel (128 threads):
+// limited by its registers, its shared memory and its 128 of the SM's 512
+// TMEM columns.  (The occupancy query reports one CTA for this kernel.)
+int tc_tile_blocks_per_sm(const void *fn, size_t smem)
+{
+    cudaFuncAttributes a{};
+    if (cudaFuncGetAttributes(&a, fn) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    const int regs = std::max(1, a.numRegs);
+    const int by_regs = 65536 / (128 * ((regs + 7) / 8 * 8));
+    const int by_smem = static_cast<int>((228 * 1024) / (smem + a.sharedSizeBytes + 1024));
+    return std::max(1, std::min({4, by_regs, by_smem}));
+}
+
 int grid_for(int64_t tiles)
 {
     const int64_t cap = int64_t(kB200Sms) * 64;
@@ -400,7 +416,7 @@ struct Builder {
         d.pitch = ((n - 1) + ((n - 1) >> 4) + 1) | 1;
         d.tiles_per_outer = (d.n_cols + d.tb - 1) / d.tb;
         d.num_tiles = d.tiles_per_outer * d.n_outer;
-        const int per_sm = std::max(1, kernel_blocks_per_sm(fn, 128, smem));
+        const int per_sm = tc_tile_blocks_per_sm(fn, smem);
         s.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(d.num_tiles, int64_t(per_sm) * sm_count(device))));
         s.has_row = false;
         s.row_fn = nullptr;
