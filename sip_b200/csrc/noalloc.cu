@@ -79,7 +79,10 @@ bool pass_radices(int n, int *r, int &count)
     }
     if (twos > 0) {
         const int s = (twos + 3) / 4, base = twos / s, extra = twos % s;
-        for (int i = 0; i < s; i++) r[count++] = 1 << (base + (i < extra ? 1 : 0));
+        for (int i = 0; i < s; i++) {
+            if (count >= kMaxStages) return false;
+            r[count++] = 1 << (base + (i < extra ? 1 : 0));
+        }
     }
     for (int p : {13, 11, 7, 5, 3}) {
         while (m % p == 0) {
@@ -153,6 +156,14 @@ bool make_pass(TileDesc &d, int &maxe, int &grid, int rp, int64_t F, int64_t row
         }
     }
     if (d.tb == 0) return false;
+    if (d.tb >= 2) {
+        // column tiles: a pitch with P mod (32/tb) = 16/tb puts a half warp's
+        // tb transforms x 16/tb elements on 16 distinct 8-byte bank pairs
+        const int m = 32 / d.tb, want = 16 / d.tb;
+        int p = pitch;
+        while (p % m != want) p++;
+        if (int64_t(d.tb) * p * 8 <= kMaxSmemBytes) d.pitch = p;
+    }
     d.xfast = 1;
     d.n_outer = rows;
     d.n_cols = F / rp;

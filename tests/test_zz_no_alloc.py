@@ -29,7 +29,9 @@ def _no_alloc(lib, x_ptr, y_ptr, n, batch, direction, stream):
 @pytest.mark.parametrize("n,batch,direction", [(32768, 4, fft.ASCEND_FFT_FORWARD),
                                                (65536, 16, fft.ASCEND_FFT_INVERSE),
                                                (3 * 2 ** 14, 5, fft.ASCEND_FFT_FORWARD),
-                                               (2 ** 20, 1, fft.ASCEND_FFT_FORWARD)])
+                                               (2 ** 20, 1, fft.ASCEND_FFT_FORWARD),
+                                               # 7 * 11 * 13 * 32: passes with odd radices
+                                               (7 * 11 * 13 * 32, 3, fft.ASCEND_FFT_INVERSE)])
 def test_no_alloc_matches_plan_path(cuda, n, batch, direction):
     import torch
 
@@ -51,6 +53,22 @@ def test_no_alloc_matches_plan_path(cuda, n, batch, direction):
         assert oracle.rel_l2(got, ref) <= tol, f"call {call}: {oracle.rel_l2(got, ref)}"
         assert oracle.rel_l2(got, oracle.c2c(x, direction == fft.ASCEND_FFT_FORWARD)) <= tol
     plan.close()
+
+
+def test_no_alloc_in_place_at_the_size_limit(cuda):
+    """input == output, length * batch exactly at the array's 2^20 limit with batch > 1:
+    the tables and the intermediate never overlap the caller's buffer."""
+    import torch
+
+    lib = fft.load_library()
+    n, batch = 65536, 16
+    rng = np.random.default_rng(7)
+    x = (rng.uniform(-1, 1, (batch, n)) + 1j * rng.uniform(-1, 1, (batch, n))).astype(np.complex64)
+    buf = torch.from_numpy(x).cuda()
+    stream = torch.cuda.current_stream()
+    assert _no_alloc(lib, buf.data_ptr(), buf.data_ptr(), n, batch, fft.ASCEND_FFT_FORWARD, stream) == fft.ACL_SUCCESS
+    torch.cuda.synchronize()
+    assert oracle.rel_l2(buf.cpu().numpy(), oracle.c2c(x, True)) <= oracle.tolerance(n)
 
 
 def test_no_alloc_rejects_sizes_beyond_the_array(cuda):
