@@ -23,11 +23,15 @@ __device__ __forceinline__ int64_t col_base(const Addr &a, int64_t o, int64_t c)
     return x;
 }
 
+// W_F^(e kc step) from the two-level table.  The exponent is below F (e < n,
+// kc < Ns, step = F / (Ns n)), and every multi-pass length F is at most 2^28
+// (transforms up to 2^27 points, Bluestein convolutions up to 2^28), so the
+// index arithmetic is exact in 32 bits.
 template <bool FWD>
 __device__ __forceinline__ float2 pass_twiddle(const TileDesc &d, int64_t e, int64_t kc)
 {
-    const int64_t m = e * kc * d.g_step;
-    const int64_t mask = (int64_t(1) << d.g_log2l) - 1;
+    const uint32_t m = static_cast<uint32_t>(e) * static_cast<uint32_t>(kc) * static_cast<uint32_t>(d.g_step);
+    const uint32_t mask = (1u << d.g_log2l) - 1u;
     const float2 w = cmul(__ldg(d.g_lo + (m & mask)), __ldg(d.g_hi + (m >> d.g_log2l)));
     return dir<FWD>(w);
 }
