@@ -389,3 +389,46 @@ def test_tma_column_tiles_and_fallback_agree(cuda, n, batch):
         assert oracle.rel_l2(outs[-1], ref) <= oracle.tolerance(n), shift
     assert np.max(np.abs(outs[0] - outs[1])) <= 1e-5 * np.max(np.abs(ref))
     plan.close()
+
+
+def test_dependent_launches_back_to_back(cuda):
+    """A chain of plans on one stream with no host synchronisation in between:
+    every kernel is launched with programmatic stream serialization and must
+    wait for the previous launch's results (and not overwrite what it still
+    reads) before touching memory.  Each link reads the previous link's output."""
+    import torch
+
+    rng = np.random.default_rng(77)
+    s = torch.cuda.Stream()
+    n2, n1, rows = 2048, 4096, 96
+    x = rng.standard_normal((rows, n1)).astype(np.float32)
+    plans = [fft.FftPlan([n1], R2C, FWD, rows, stream=s), fft.FftPlan([n1], C2R, INV, rows, stream=s),
+             fft.FftPlan([rows // 2, n1 * 2], C2C, FWD, 1, stream=s),
+             fft.FftPlan([65536], C2C, INV, rows * n1 // 65536, stream=s),
+             fft.FftPlan([n2], C2C, FWD, rows * n1 // n2, fft.ASCEND_FFT_VERTICAL, stream=s)]
+    xd = torch.from_numpy(x).cuda()
+    X = torch.empty((rows, n1 // 2 + 1), dtype=torch.complex64, device="cuda")
+    y = torch.empty_like(xd)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        for _ in range(3):  # repeated, so later launches overlap earlier ones' tails
+            plans[0](xd, X)
+            plans[1](X, y)
+            z = torch.complex(y, torch.zeros_like(y)).reshape(rows // 2, n1 * 2)
+            z1 = torch.empty_like(z)
+            plans[2](z.reshape(1, rows // 2, n1 * 2), z1.reshape(1, rows // 2, n1 * 2))
+            z2 = torch.empty_like(z1)
+            plans[3](z1.reshape(-1, 65536), z2.reshape(-1, 65536))
+            z3 = torch.empty_like(z2)
+            plans[4](z2.reshape(n2, -1), z3.reshape(n2, -1))
+    s.synchronize()
+    for p in plans:
+        assert fft.asdFftSynchronize(p.handle) == fft.ACL_SUCCESS
+    X_ref = oracle.r2c(x, True)
+    y_ref = oracle.c2r(X_ref, n1, False)
+    z_ref = oracle.c2c(y_ref.reshape(1, rows // 2, n1 * 2).astype(np.complex128), True, ndim=2)
+    z_ref = oracle.c2c(z_ref.reshape(-1, 65536), False)
+    z_ref = oracle.c2c(z_ref.reshape(n2, -1).T, True).T
+    assert oracle.rel_l2(z3.reshape(n2, -1).cpu().numpy(), z_ref) <= 5 * oracle.tolerance(65536)
+    for p in plans:
+        p.close()
