@@ -61,7 +61,7 @@ struct ColOut {
 }  // namespace
 
 template <class Q, int T, int TB, bool FWD>
-__global__ void __launch_bounds__(TB *T, (TB * T <= 256) ? 2 : 1)
+__global__ void __launch_bounds__(TB *T, (TB * T <= 256) ? 3 : 1)
     col_pipe_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ TileDesc d, int *err)
 {
     pdl_enter();
@@ -138,12 +138,14 @@ ColPipeEntry col_entry()
 }
 
 // Engines with 16 points per thread (the same radix sequences as the
-// power-of-two row engines), TB = min(16, 512 / threads per transform).
+// power-of-two row engines); TB columns per tile as the planner chooses them
+// (CTAs of at most 256 threads, three per SM, while TB stays >= 4, i.e. rows
+// of at least one 32-byte sector; 512 threads for 2048 points).
 const std::vector<ColPipeEntry> &col_registry()
 {
     static const std::vector<ColPipeEntry> r = {
-        col_entry<Seq<16, 4>, 4, 16>(),     col_entry<Seq<16, 8>, 8, 16>(),    col_entry<Seq<16, 16>, 16, 16>(),
-        col_entry<Seq<16, 16, 2>, 32, 16>(), col_entry<Seq<16, 16, 4>, 64, 8>(), col_entry<Seq<16, 16, 8>, 128, 4>(),
+        col_entry<Seq<16, 4>, 4, 16>(),     col_entry<Seq<16, 8>, 8, 16>(),   col_entry<Seq<16, 16>, 16, 16>(),
+        col_entry<Seq<16, 16, 2>, 32, 8>(), col_entry<Seq<16, 16, 4>, 64, 4>(), col_entry<Seq<16, 16, 8>, 128, 4>(),
     };
     return r;
 }

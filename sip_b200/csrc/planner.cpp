@@ -77,9 +77,12 @@ bool choose_cfg(int n, bool column, int64_t ncols, TileCfg &c, std::string &err,
     c.pitch = pitch_for(n);
     const int64_t bytes_per = int64_t(c.pitch) * 8;
     if (column) {
+        // column tiles: at most 256 threads while that keeps >= 4 columns (32-byte
+        // row runs), so that several CTAs share an SM; else up to max_threads
+        const int col_threads = (4 * c.tpt <= 256) ? 256 : max_threads;
         c.tb = 0;
         for (int tb = kColTile; tb >= 1; tb /= 2) {
-            if (tb * c.tpt <= max_threads && tb * bytes_per <= kMaxSmemBytes) {
+            if (tb * c.tpt <= col_threads && tb * bytes_per <= kMaxSmemBytes) {
                 c.tb = tb;
                 break;
             }
