@@ -267,6 +267,17 @@ __device__ __forceinline__ bool batch_dep_wait(const BatchSeg *segs, int *done, 
     return false;
 }
 
+// The tile descriptor of the item a CTA computes and of the one it prefetches
+// sit in shared memory (copied once per item), so the stage loops read them
+// with shared-memory latency instead of re-reading the segment list.
+__device__ __forceinline__ void copy_desc(TileDesc *dst, const TileDesc &src)
+{
+    static_assert(sizeof(TileDesc) % 8 == 0, "descriptor copied as 8-byte words");
+    const uint64_t *s = reinterpret_cast<const uint64_t *>(&src);
+    uint64_t *d = reinterpret_cast<uint64_t *>(dst);
+    for (int i = threadIdx.x; i < static_cast<int>(sizeof(TileDesc) / 8); i += blockDim.x) d[i] = __ldg(s + i);
+}
+
 template <int MAXE, bool FWD>
 __global__ void __launch_bounds__(kBatchBlock, 2)
     batch_fft_kernel(const BatchSeg *__restrict__ segs, const int2 *__restrict__ items, int nitems, int *counter,
@@ -274,6 +285,7 @@ __global__ void __launch_bounds__(kBatchBlock, 2)
 {
     extern __shared__ float2 sm[];
     __shared__ int s_item, s_pref, s_ok;
+    __shared__ TileDesc s_desc[2];  // [i & 1]: the item computed in iteration i
     const int tid = threadIdx.x;
     // dequeue the first item; prefetch it when it is ready to read
     if (tid == 0) {
@@ -287,14 +299,18 @@ __global__ void __launch_bounds__(kBatchBlock, 2)
     __syncthreads();
     int w = s_item;
     bool pref = s_pref != 0;
+    if (w < nitems) copy_desc(&s_desc[0], segs[items[w].x].d);
+    __syncthreads();
     if (w < nitems && pref) {
         const int2 it = items[w];
         const BatchSeg &sg = segs[it.x];
-        issue_tile_c2c(sg.d, static_cast<const char *>(bufs.p[sg.in_buf]) + sg.in_off, sm, it.y);
+        issue_tile_c2c(s_desc[0], static_cast<const char *>(bufs.p[sg.in_buf]) + sg.in_off, sm, it.y);
     }
     cp_async_commit();
     for (int i = 0; w < nitems; i++) {
         float2 *cur = sm + (i & 1) * span;
+        const TileDesc &d = s_desc[i & 1];
+        TileDesc &dn = s_desc[(i + 1) & 1];
         // dequeue the next item and prefetch it into the other buffer when possible
         __syncthreads();  // everyone has read s_item / s_pref of the current item
         if (tid == 0) {
@@ -308,10 +324,13 @@ __global__ void __launch_bounds__(kBatchBlock, 2)
         __syncthreads();
         const int wn = s_item;
         const bool pref_n = s_pref != 0;
+        // the previous iteration's item, whose descriptor slot this is, has finished
+        if (wn < nitems) copy_desc(&dn, segs[items[wn].x].d);
+        __syncthreads();
         if (wn < nitems && pref_n) {
             const int2 itn = items[wn];
             const BatchSeg &nsg = segs[itn.x];
-            issue_tile_c2c(nsg.d, static_cast<const char *>(bufs.p[nsg.in_buf]) + nsg.in_off, sm + ((i + 1) & 1) * span,
+            issue_tile_c2c(dn, static_cast<const char *>(bufs.p[nsg.in_buf]) + nsg.in_off, sm + ((i + 1) & 1) * span,
                            itn.y);
         }
         cp_async_commit();
@@ -331,7 +350,7 @@ __global__ void __launch_bounds__(kBatchBlock, 2)
         if (ok) {
             // a Bluestein segment runs its convolution FFTs in both directions; the
             // other direction is conj(DFT(conj(y))) around this kernel's stages
-            process_tile<MAXE, FWD>(sg.d, in, out, it.y, cur, sg.fwd != (FWD ? 1 : 0), pref);
+            process_tile<MAXE, FWD>(d, in, out, it.y, cur, sg.fwd != (FWD ? 1 : 0), pref);
             if (tid == 0) {
                 __threadfence();
                 atomicAdd(done + it.x, 1);

@@ -178,13 +178,66 @@ __device__ __forceinline__ float2 *bbuf(float2 *work, float2 *work2)
     return (PP && B % 2 == 0) ? work2 : work;
 }
 
+// Barrier between two steps that touch only the work rows of the CTA's own
+// transforms.  With warp-local lanes (WL: the T <= 32 threads of a transform
+// are consecutive lanes of one warp, as in the row kernels) a transform's
+// work row is written and read by its own warp only, so the warp's barrier
+// suffices; stage 0's gather still ends with a CTA barrier, because the
+// staged input rows alias the work rows of other warps' transforms.
+template <int WL>
+__device__ __forceinline__ void row_sync()
+{
+    if constexpr (WL > 0)
+        __syncwarp();
+    else
+        __syncthreads();
+}
+
+// Last stage of radix 2 as warp-shuffle butterflies.  When stage S-2 has one
+// butterfly per thread and T = 2 Ns(S-2) <= 32 (warp-local lanes), element
+// j < N/2 of the last boundary sits in register j / H of lane j mod H and
+// element j + N/2 in the same register of lane H + j mod H (H = T/2), so the
+// butterfly X[j] = a + w^j b, X[j + N/2] = a - w^j b pairs lanes (lane,
+// lane ^ H) register by register.  Every lane multiplies its operand by a
+// stage-table entry (w^j in the upper lane, entry 0 = 1 in the lower one, so
+// both run the same instructions), swaps the product with its partner and
+// keeps one output: lower a + w^j b, upper a - w^j b.  The stage needs no
+// shared memory and no barrier; stores of one register cover two runs of H
+// consecutive bins.
+template <class Q, int T, int WL>
+struct ShflLast {
+    static constexpr bool ok =
+        WL == 2 && Q::S >= 2 && Q::r[Q::S - 1] == 2 && T == 2 * Q::ns(Q::S - 2) && Q::N / Q::r[Q::S - 2] == T;
+};
+
+template <class Q, int T, bool FWD, class DstL>
+__device__ __forceinline__ void shfl_last(const float2 *v, const DstL &dst, int lane, bool active,
+                                          const float2 *__restrict__ stw)
+{
+    constexpr int S = Q::S - 1, RP = Q::r[S - 1], H = T / 2, HALF = Q::N / 2;
+    const bool up = (lane & H) != 0;
+    const int lo = lane & (H - 1);
+    const int sel = up ? -1 : 0;
+    const float sg = up ? -1.f : 1.f;
+    const float2 *t = stw + Q::tw_off(S);
+#pragma unroll
+    for (int r = 0; r < RP; r++) {
+        const int j = lo + r * H;
+        const float2 q = cmul(v[r], dir<FWD>(__ldg(t + (j & sel))));
+        const float px = __shfl_xor_sync(0xffffffffu, q.x, H);
+        const float py = __shfl_xor_sync(0xffffffffu, q.y, H);
+        if (active) dst(j + (up ? HALF : 0), make_float2(fmaf(sg, q.x, px), fmaf(sg, q.y, py)));
+    }
+}
+
 // Stage S of the static FFT; stage 0 reads src0 (the staging rows, which
 // alias the work buffer), the last stage writes dstL.
-template <class Q, int T, class PD, bool PP, bool FWD, int S, class Src0, class DstL>
+template <class Q, int T, class PD, bool PP, int WL, bool FWD, int S, class Src0, class DstL>
 __device__ __forceinline__ void srun(float2 *v, float2 *work, float2 *work2, const Src0 &src0, const DstL &dstL,
                                      bool dst_in_place, int lane, bool active, const float2 *stw)
 {
-    constexpr bool last = S == Q::S - 1;
+    constexpr bool shfl = ShflLast<Q, T, WL>::ok && S == Q::S - 2;
+    constexpr bool last = S == Q::S - 1 || shfl;
     if constexpr (S == 0)
         sgather<Q, 0, T, FWD>(v, src0, lane, active, stw);
     else
@@ -192,13 +245,26 @@ __device__ __forceinline__ void srun(float2 *v, float2 *work, float2 *work2, con
     if constexpr (last) {
         // an in-place destination is the work row: wait while it is still gathered from
         constexpr bool src_is_work = S == 0 || !(PP && (S - 1) % 2 == 0);
-        if (dst_in_place && src_is_work) __syncthreads();
-        sscatter<Q, S, T>(v, dstL, lane, active);
+        if (dst_in_place && src_is_work) {
+            if constexpr (S == 0)
+                __syncthreads();
+            else
+                row_sync<WL>();
+        }
+        if constexpr (shfl)
+            shfl_last<Q, T, FWD>(v, dstL, lane, active, stw);
+        else
+            sscatter<Q, S, T>(v, dstL, lane, active);
     } else {
-        if constexpr (!PP) __syncthreads();
+        if constexpr (!PP) {
+            if constexpr (S == 0)
+                __syncthreads();
+            else
+                row_sync<WL>();
+        }
         sscatter<Q, S, T>(v, BoundaryRow<PD, S>{bbuf<PP, S>(work, work2)}, lane, active);
-        __syncthreads();
-        srun<Q, T, PD, PP, FWD, S + 1>(v, work, work2, src0, dstL, dst_in_place, lane, active, stw);
+        row_sync<WL>();
+        srun<Q, T, PD, PP, WL, FWD, S + 1>(v, work, work2, src0, dstL, dst_in_place, lane, active, stw);
     }
 }
 
@@ -396,8 +462,15 @@ struct FusedC2R {
     }
 };
 
-template <class Q, int T, class PD = Pads<>, bool PP = false>
+// WL = 1: the T threads of a transform are consecutive lanes of one warp (row
+// kernels with T <= 32), so barriers that guard only a transform's own work
+// row are warp barriers; WL = 2 also runs a last radix-2 stage as
+// warp-shuffle butterflies where ShflLast applies.  WL = 0 (the column and
+// double-buffered tile kernels, which spread a transform's threads over the
+// CTA) keeps CTA barriers.
+template <class Q, int T, class PD = Pads<>, bool PP = false, int WL = 0>
 struct StaticEngine {
+    static_assert(WL == 0 || (T <= 32 && 32 % T == 0), "warp-local lanes need T dividing 32");
     static constexpr bool kPingPong = PP;  // a third shared-memory buffer holds the even boundaries
     static constexpr int kMaxThreads = T <= 256 ? 256 : T;
     // 3 CTAs per SM (<= 80 registers) unless a thread holds more than 16 points
@@ -407,7 +480,7 @@ struct StaticEngine {
                                                bool dst_in_place, int lane, bool active, float2 *work2 = nullptr)
     {
         float2 v[static_maxv<Q, T>()];
-        srun<Q, T, PD, PP, FWD, 0>(v, work, work2, src0, dstL, dst_in_place, lane, active, d.stw);
+        srun<Q, T, PD, PP, WL, FWD, 0>(v, work, work2, src0, dstL, dst_in_place, lane, active, d.stw);
     }
 
     template <bool FWD, class Src0>
@@ -419,11 +492,11 @@ struct StaticEngine {
             constexpr int V = static_maxv<Q, T>() > 2 * F::R ? static_maxv<Q, T>() : 2 * F::R;
             float2 v[V];
             prefix<FWD, 0>(v, work, work2, src0, lane, active, d.stw);
-            __syncthreads();
+            row_sync<WL>();
             F::run(v, bbuf<PP, Q::S - 2>(work, work2), y, lane, active, d.stw, d.tw);
         } else {
             run<FWD>(d, work, src0, SmemRow{work}, true, lane, active, work2);
-            __syncthreads();
+            row_sync<WL>();
             if (active) r2c_post_row<FWD>(work, y, d.n, lane, d.tpt, d.tw);
         }
     }
@@ -454,8 +527,8 @@ struct StaticEngine {
                     w(j1 * R + r, v[R + r]);
                 }
             }
-            __syncthreads();
-            srun<Q, T, PD, PP, FWD, 1>(v, work, work2, SmemRow{work}, dstL, false, lane, active, d.stw);
+            row_sync<WL>();
+            srun<Q, T, PD, PP, WL, FWD, 1>(v, work, work2, SmemRow{work}, dstL, false, lane, active, d.stw);
         } else {
             run<FWD>(d, work, C2RPre<FWD>{x, d.n, d.tw}, dstL, false, lane, active, work2);
         }
@@ -471,9 +544,14 @@ struct StaticEngine {
                 sgather<Q, 0, T, FWD>(v, src0, lane, active, stw);
             else
                 sgather<Q, S, T, FWD>(v, BoundaryRow<PD, S - 1>{bbuf<PP, S - 1>(work, work2)}, lane, active, stw);
-            if constexpr (!PP) __syncthreads();
+            if constexpr (!PP) {
+                if constexpr (S == 0)
+                    __syncthreads();
+                else
+                    row_sync<WL>();
+            }
             sscatter<Q, S, T>(v, BoundaryRow<PD, S>{bbuf<PP, S>(work, work2)}, lane, active);
-            if constexpr (S + 1 < Q::S - 1) __syncthreads();
+            if constexpr (S + 1 < Q::S - 1) row_sync<WL>();
             prefix<FWD, S + 1>(v, work, work2, src0, lane, active, stw);
         }
     }

@@ -79,7 +79,9 @@ constexpr bool pads_fit()
     return true;
 }
 
-template <class Q, int T, class PD = Pads<>, bool PP = false>
+// SH: the row kernels run a last radix-2 stage as warp-shuffle butterflies
+// (StaticEngine WL = 2) where the engine's shape allows it
+template <class Q, int T, class PD = Pads<>, bool PP = false, bool SH = false>
 StaticKernel make_entry(int io_mask = 7)
 {
     static_assert(pads_fit<Q, PD>(), "padded work row exceeds the planner's pitch");
@@ -89,7 +91,10 @@ StaticKernel make_entry(int io_mask = 7)
     e.nstages = Q::S;
     for (int s = 0; s < Q::S; s++) e.radix[s] = Q::r[s];
     e.tpt = T;
-    using E = StaticEngine<Q, T, PD, PP>;
+    // row kernels: a transform of T <= 32 threads lives in one warp
+    using E = StaticEngine<Q, T, PD, PP, (T <= 32 ? (SH ? 2 : 1) : 0)>;
+    static_assert(!SH || ShflLast<Q, T, 2>::ok, "no warp-shuffle last stage for this engine");
+    using EDb = StaticEngine<Q, T, PD, PP>;
     e.row_bufs = PP ? 3 : 2;
     e.fn[1][0] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, true, IO_C2C>);
     e.fn[1][1] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, true, IO_R2C_PACKED>);
@@ -98,8 +103,8 @@ StaticKernel make_entry(int io_mask = 7)
     e.fn[0][1] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, false, IO_R2C_PACKED>);
     e.fn[0][2] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, false, IO_C2R_PACKED>);
     if constexpr (!PP) {  // the double-buffered tile kernel has no ping-pong area
-        e.db[1] = reinterpret_cast<const void *>(static_db_kernel<E, true>);
-        e.db[0] = reinterpret_cast<const void *>(static_db_kernel<E, false>);
+        e.db[1] = reinterpret_cast<const void *>(static_db_kernel<EDb, true>);
+        e.db[0] = reinterpret_cast<const void *>(static_db_kernel<EDb, false>);
     }
     return e;
 }
@@ -110,7 +115,12 @@ const std::vector<StaticKernel> &registry()
         make_entry<Seq<16, 4>, 4>(),            // 64
         make_entry<Seq<16, 8>, 8>(),            // 128
         make_entry<Seq<16, 16>, 16>(),          // 256
-        make_entry<Seq<16, 16, 2>, 32>(),       // 512
+        // 512: C2C with a shared-memory last stage; the packed halves of the
+        // 1024-point real transforms with warp-shuffle butterflies in the last
+        // radix-2 stage (measured: C2R 1024 7 % and R2C 1024 3 % faster, C2C
+        // 512 3 % slower than the shared-memory stage)
+        make_entry<Seq<16, 16, 2>, 32>(1),
+        make_entry<Seq<16, 16, 2>, 32, Pads<>, false, true>(6),
         make_entry<Seq<16, 16, 4>, 64>(),       // 1024
         // 2048, C2R: pre-twiddle fused into the radix-8 first stage, ping-pong
         // work rows (4 CTAs per SM instead of 6, measured 3 % faster; the R2C

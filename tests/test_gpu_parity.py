@@ -261,11 +261,14 @@ def test_stream_and_sync(cuda):
     plan.close()
 
 
-@pytest.mark.parametrize("typ,n", [(C2C, 1024), (C2C, 4096), (R2C, 4096), (R2C, 3000), (C2R, 3000), (C2R, 4096)])
+@pytest.mark.parametrize("typ,n", [(C2C, 1024), (C2C, 4096), (R2C, 4096), (R2C, 3000), (C2R, 3000), (C2R, 4096),
+                                   (C2C, 512), (R2C, 1024), (C2R, 1024), (R2C, 256), (C2R, 128)])
 def test_pipelined_and_generic_kernels_agree(cuda, typ, n):
     """A 16-byte aligned source takes the TMA-pipelined row kernel; an 8-byte
     aligned one (offset by one element through the aclTensor offset) takes the
-    generic tile kernel.  Both must give the oracle's result."""
+    generic tile kernel.  Both must give the oracle's result.  The 1024-point
+    real transforms run the 512-point engine whose last radix-2 stage is
+    warp-shuffle butterflies; 128..512-point engines use warp barriers."""
     import torch
 
     rng = np.random.default_rng(n + typ)
