@@ -284,54 +284,50 @@ __global__ void __launch_bounds__(kBatchBlock, 2)
                      int *done, BatchBufs bufs, int *err, int64_t span)
 {
     extern __shared__ float2 sm[];
-    __shared__ int s_item, s_pref, s_ok;
-    __shared__ TileDesc s_desc[2];  // [i & 1]: the item computed in iteration i
+    // [i & 1]: the item computed in iteration i (the next item's slots are
+    // written while the current item's are still read)
+    __shared__ int s_item[2], s_pref[2], s_ok;
+    __shared__ TileDesc s_desc[2];
     const int tid = threadIdx.x;
-    // dequeue the first item; prefetch it when it is ready to read
-    if (tid == 0) {
-        s_item = atomicAdd(counter, 1);
-        s_pref = 0;
-        if (s_item < nitems) {
-            const BatchSeg &sg = segs[items[s_item].x];
-            s_pref = sg.d.io == IO_C2C && batch_dep_done(segs, done, sg);
+    auto dequeue = [&](int slot) {
+        const int w = atomicAdd(counter, 1);
+        int pf = 0;
+        if (w < nitems) {
+            const BatchSeg &sg = segs[items[w].x];
+            pf = sg.d.io == IO_C2C && batch_dep_done(segs, done, sg);
         }
-    }
+        s_item[slot] = w;
+        s_pref[slot] = pf;
+    };
+    // dequeue the first item; prefetch it when it is ready to read
+    if (tid == 0) dequeue(0);
     __syncthreads();
-    int w = s_item;
-    bool pref = s_pref != 0;
-    if (w < nitems) copy_desc(&s_desc[0], segs[items[w].x].d);
-    __syncthreads();
-    if (w < nitems && pref) {
+    int w = s_item[0];
+    bool pref = s_pref[0] != 0;
+    if (w < nitems) {
         const int2 it = items[w];
         const BatchSeg &sg = segs[it.x];
-        issue_tile_c2c(s_desc[0], static_cast<const char *>(bufs.p[sg.in_buf]) + sg.in_off, sm, it.y);
+        copy_desc(&s_desc[0], sg.d);
+        if (pref) issue_tile_c2c(sg.d, static_cast<const char *>(bufs.p[sg.in_buf]) + sg.in_off, sm, it.y);
     }
     cp_async_commit();
     for (int i = 0; w < nitems; i++) {
+        const int nx = (i + 1) & 1;
         float2 *cur = sm + (i & 1) * span;
-        const TileDesc &d = s_desc[i & 1];
-        TileDesc &dn = s_desc[(i + 1) & 1];
-        // dequeue the next item and prefetch it into the other buffer when possible
-        __syncthreads();  // everyone has read s_item / s_pref of the current item
-        if (tid == 0) {
-            s_item = atomicAdd(counter, 1);
-            s_pref = 0;
-            if (s_item < nitems) {
-                const BatchSeg &nsg = segs[items[s_item].x];
-                s_pref = nsg.d.io == IO_C2C && batch_dep_done(segs, done, nsg);
-            }
-        }
+        // dequeue the next item, copy its descriptor and prefetch it into the
+        // other buffer when its producer has finished (the previous iteration's
+        // item, whose slots and buffer these are, ended with a barrier)
+        if (tid == 0) dequeue(nx);
         __syncthreads();
-        const int wn = s_item;
-        const bool pref_n = s_pref != 0;
-        // the previous iteration's item, whose descriptor slot this is, has finished
-        if (wn < nitems) copy_desc(&dn, segs[items[wn].x].d);
-        __syncthreads();
-        if (wn < nitems && pref_n) {
+        const int wn = s_item[nx];
+        const bool pref_n = s_pref[nx] != 0;
+        if (wn < nitems) {
             const int2 itn = items[wn];
             const BatchSeg &nsg = segs[itn.x];
-            issue_tile_c2c(dn, static_cast<const char *>(bufs.p[nsg.in_buf]) + nsg.in_off, sm + ((i + 1) & 1) * span,
-                           itn.y);
+            copy_desc(&s_desc[nx], nsg.d);
+            if (pref_n)
+                issue_tile_c2c(nsg.d, static_cast<const char *>(bufs.p[nsg.in_buf]) + nsg.in_off, sm + nx * span,
+                               itn.y);
         }
         cp_async_commit();
 
@@ -350,7 +346,7 @@ __global__ void __launch_bounds__(kBatchBlock, 2)
         if (ok) {
             // a Bluestein segment runs its convolution FFTs in both directions; the
             // other direction is conj(DFT(conj(y))) around this kernel's stages
-            process_tile<MAXE, FWD>(d, in, out, it.y, cur, sg.fwd != (FWD ? 1 : 0), pref);
+            process_tile<MAXE, FWD>(s_desc[i & 1], in, out, it.y, cur, sg.fwd != (FWD ? 1 : 0), pref);
             if (tid == 0) {
                 __threadfence();
                 atomicAdd(done + it.x, 1);
