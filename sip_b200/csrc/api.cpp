@@ -686,7 +686,7 @@ int32_t asdFftPlanLaunchCount(void *handle)
     std::lock_guard<std::mutex> lock(p->mu);
     int32_t n = 0;
     for (const auto &s : p->steps) {
-        if (s.kind == sipfft::StepKind::kTile)
+        if (s.kind == sipfft::StepKind::kTile || s.kind == sipfft::StepKind::kTranspose)
             n += 1;
         else
             n += static_cast<int32_t>((s.rows + 65534) / 65535);

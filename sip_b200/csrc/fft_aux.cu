@@ -5,6 +5,9 @@
 // reference's even-length path (core/fft/fftcore/include/fftcore/fft_r2c_core.h:21-24,
 // A/B tables in fft_core_common_func.cpp:569-673), written as the split
 // X[k] = E[k] + w^k O[k] with E, O recovered from the packed spectrum Z.
+#include <algorithm>
+
+#include "async_copy.cuh"
 #include "codelets.cuh"
 #include "sipfft_internal.h"
 
@@ -224,6 +227,50 @@ cudaError_t launch_blue_post(const float2 *a, void *out, int64_t rows, int64_t n
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+// ------------------------------------------------------------------------------------ transpose
+// Out-of-place transpose of a batch of complex matrices through 32 x 32 tiles
+// in shared memory: a warp reads 32 consecutive elements of one row (256
+// bytes) and writes 32 consecutive elements of one output row.  The padded
+// tile row (33 elements) keeps the column reads at two wavefronts per warp.
+// Persistent grid; each CTA walks tiles (matrix, tile row, tile column).
+__global__ void __launch_bounds__(256) transpose_kernel(const float2 *__restrict__ in, float2 *__restrict__ out,
+                                                        int64_t rows, int64_t cols, int64_t tiles_r, int64_t tiles_c,
+                                                        int64_t ntiles)
+{
+    __shared__ float2 t[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int64_t per = tiles_r * tiles_c;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t b = tile / per, rem = tile - b * per;
+        const int64_t r0 = (rem / tiles_c) * 32, c0 = (rem % tiles_c) * 32;
+        const float2 *src = in + b * rows * cols;
+        float2 *dst = out + b * rows * cols;
+#pragma unroll
+        for (int i = ty; i < 32; i += 8) {
+            const int64_t r = r0 + i, c = c0 + tx;
+            if (r < rows && c < cols) t[i][tx] = src[r * cols + c];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = ty; i < 32; i += 8) {
+            const int64_t c = c0 + i, r = r0 + tx;
+            if (c < cols && r < rows) st_stream(dst + c * rows + r, t[tx][i]);
+        }
+        __syncthreads();
+    }
+}
+
+cudaError_t launch_transpose(const float2 *in, float2 *out, int64_t batch, int64_t rows, int64_t cols, int device,
+                             cudaStream_t st)
+{
+    if (batch <= 0 || rows <= 0 || cols <= 0 || in == out) return cudaErrorInvalidValue;
+    const int64_t tiles_r = (rows + 31) / 32, tiles_c = (cols + 31) / 32;
+    const int64_t ntiles = batch * tiles_r * tiles_c;
+    const int64_t grid = std::min<int64_t>(ntiles, int64_t(sm_count(device)) * 8);
+    transpose_kernel<<<static_cast<int>(grid), 256, 0, st>>>(in, out, rows, cols, tiles_r, tiles_c, ntiles);
+    return cudaGetLastError();
 }
 
 }  // namespace sipfft

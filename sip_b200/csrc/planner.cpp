@@ -356,13 +356,60 @@ struct Builder {
         // single-tile tensor-core kernel, several times slower than the double-buffered FP32 passes
         if (in_multipass || p.fft_type == 0x30 || !(io == IO_C2C || io == IO_R2C_PACKED || io == IO_C2R_PACKED))
             return true;
+        const int form = tc_form(n);
+        return form == 1 || form == 2 ? add_tc_variant(s, form) : true;
+    }
+
+    // Stage arithmetic of a length-n step: 0 FP32, 1 FP16 x3, 2 BF16 x3 (in
+    // precision mode 3, per length, what the autotuner measured fastest).
+    int tc_form(int64_t n) const
+    {
         int form = p.precision;
         if (form == 3) {
-            // per length, the arithmetic the autotuner measured fastest
             TuneChoice t;
             form = tuned_choice(n, t) ? t.precision : 0;
         }
-        return form == 1 || form == 2 ? add_tc_variant(s, form) : true;
+        return form;
+    }
+
+    // Out-of-place transpose of `batch` matrices rows x cols -> cols x rows.
+    void add_transpose(int64_t batch, int64_t rows, int64_t cols, Buf src, Buf dst, const std::string &what)
+    {
+        Step s;
+        s.kind = StepKind::kTranspose;
+        s.src = src;
+        s.dst = dst;
+        s.t_batch = batch;
+        s.t_rows = rows;
+        s.t_cols = cols;
+        s.what = what;
+        p.steps.push_back(s);
+    }
+
+    // Tensor-core form of a strided C2C axis [outer][n][inner] whose length has
+    // the warp-specialised row pipeline (1024, 2048, 4096 points): transpose the
+    // axis into contiguous rows in workspace, run the rows on the pipeline,
+    // transpose back.  Three HBM round trips instead of one, but the row
+    // pipeline keeps the tensor cores fed where the single-tile tensor-core
+    // kernel on column tiles is latency-bound (the reference runs its strided
+    // axes through explicit Transpose steps as well, core/fft/fft_api.cpp:527-697).
+    bool add_tc_strided(int64_t n, int64_t outer, int64_t inner, Buf src, Buf dst)
+    {
+        const Buf a = free_ws({src, dst}), b = free_ws({src, dst, a});
+        const size_t bytes = size_t(outer) * size_t(n) * size_t(inner) * sizeof(float2);
+        need_ws(a, bytes);
+        need_ws(b, bytes);
+        std::ostringstream w;
+        w << "C2C axis n=" << n << " outer=" << outer << " inner=" << inner;
+        add_transpose(outer, n, inner, src, a, w.str() + ": transpose to rows");
+        const float2 *tw = table(n, n);
+        if (!tw) return false;
+        Addr ra{0, n, 1, 0, 0};
+        if (!add_tile(IO_C2C, static_cast<int>(n), 1, tw, false, 1, outer * inner, ra, ra, a, b,
+                      w.str() + ": rows"))
+            return false;
+        add_transpose(outer, inner, n, b, dst, w.str() + ": transpose back");
+        return true;
     }
 
     // Tensor-core split-precision form of a tile step (lengths with a
@@ -730,6 +777,10 @@ struct Builder {
             err = "strided axis of length " + std::to_string(n) + " has a prime factor above 13";
             return false;
         }
+        TcConfig tcc;
+        const int form = tc_form(n);
+        if ((form == 1 || form == 2) && !in_multipass && p.fft_type != 0x30 && tc_rows_config(static_cast<int>(n), tcc))
+            return add_tc_strided(n, outer, inner, src, dst);
         TileCfg c;
         if (n > kMaxStridedTile || !choose_cfg(static_cast<int>(n), true, inner, c, err)) {
             // longer strided axes: multi-pass Stockham with 16-column tiles along the

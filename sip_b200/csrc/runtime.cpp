@@ -334,6 +334,10 @@ cudaError_t execute_steps(const Plan &p, const std::vector<Step> &steps, const v
                 e = launch_blue_post(static_cast<const float2 *>(src), dst, s.rows, s.d.blue_n, s.m, s.dst_dist,
                                      s.d.blue_kind, s.d.chirp, st);
                 break;
+            case StepKind::kTranspose:
+                e = launch_transpose(static_cast<const float2 *>(src), static_cast<float2 *>(dst), s.t_batch, s.t_rows,
+                                     s.t_cols, p.device, st);
+                break;
         }
         if (e != cudaSuccess) return e;
     }

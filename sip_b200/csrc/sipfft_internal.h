@@ -128,6 +128,9 @@ cudaError_t launch_blue_pre(const void *in, float2 *a, int64_t rows, int64_t n, 
 cudaError_t launch_point_mul(float2 *b, const float2 *bmul, int64_t rows, int64_t m, cudaStream_t st);
 cudaError_t launch_blue_post(const float2 *a, void *out, int64_t rows, int64_t n, int64_t m, int64_t out_dist,
                              int kind, const float2 *chirp, cudaStream_t st);
+// out[b][c][r] = in[b][r][c] for `batch` matrices of rows x cols complex values
+cudaError_t launch_transpose(const float2 *in, float2 *out, int64_t batch, int64_t rows, int64_t cols, int device,
+                             cudaStream_t st);
 
 // A device twiddle table shared between plans (the reference's FFTensorCache,
 // core/fft/utils/fftensor_cache.cpp:55-92, keeps coefficient tensors alive
@@ -161,7 +164,9 @@ constexpr int kWsSlots = 4;
 // kBluePre / kPointMul / kBluePost: the element-wise stages of a Bluestein
 // transform whose convolution length M is too long for one CTA (the M-point
 // FFTs between them are multi-pass tile steps).
-enum class StepKind : int { kTile = 0, kR2CPost = 1, kC2RPre = 2, kBluePre = 3, kPointMul = 4, kBluePost = 5 };
+enum class StepKind : int {
+    kTile = 0, kR2CPost = 1, kC2RPre = 2, kBluePre = 3, kPointMul = 4, kBluePost = 5, kTranspose = 6
+};
 
 struct Step {
     StepKind kind = StepKind::kTile;
@@ -191,6 +196,8 @@ struct Step {
     const float2 *tc_tw = nullptr;
     // kR2CPost / kC2RPre
     int64_t rows = 0, m = 0, src_dist = 0, dst_dist = 0;
+    // kTranspose: t_batch matrices of t_rows x t_cols complex values -> t_cols x t_rows
+    int64_t t_batch = 0, t_rows = 0, t_cols = 0;
     const float2 *lo = nullptr, *hi = nullptr;
     int log2l = 0;
     std::string what;  // human-readable description (plan dump)

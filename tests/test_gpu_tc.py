@@ -106,7 +106,8 @@ def test_c2c_vertical_columns(cuda, precision):
     rng = np.random.default_rng(3)
     x = _rand_complex(rng, (n, batch))
     y, desc = _run([n], C2C, FWD, batch, x, precision, fft.ASCEND_FFT_VERTICAL)
-    assert "tensor-core" in desc and " tile " in desc, desc
+    # the strided axis is transposed into rows for the row pipeline and back
+    assert "tensor-core" in desc and " rows " in desc and desc.count("transpose") == 2, desc
     assert oracle.rel_l2(y, oracle.c2c(x.T, True).T) <= oracle.tolerance(n)
 
 
@@ -158,6 +159,32 @@ def test_2d_2048(cuda, precision):
     y, desc = _run([2048, 2048], C2C, FWD, 2, x, precision)
     assert desc.count("tensor-core") == 2, desc
     assert oracle.rel_l2(y, oracle.c2c(x, True, ndim=2)) <= oracle.tolerance(2048 * 2048)
+
+
+@pytest.mark.parametrize("precision", MODES, ids=["fp16x3", "bf16x3"])
+@pytest.mark.parametrize("direction", [FWD, INV], ids=["fwd", "inv"])
+def test_strided_axes_through_transposes(cuda, direction, precision):
+    """Strided axes of 1024, 2048 and 4096 points run as transpose -> tensor-core
+    row pipeline -> transpose (column counts that are not multiples of the 32 x 32
+    transpose tile, several outer blocks, the R2C and C2R column passes)."""
+    rng = np.random.default_rng(77 + direction)
+    f = direction == FWD
+    x = _rand_complex(rng, (3, 1024, 96))
+    y, desc = _run([1024, 96], C2C, direction, 3, x, precision)
+    assert desc.count("transpose") == 2 and desc.count("tensor-core") == 1, desc  # 96-point rows stay FP32
+    assert oracle.rel_l2(y, oracle.c2c(x, f, ndim=2)) <= oracle.tolerance(1024 * 96)
+    v = _rand_complex(rng, (2, 3, 4096, 40))
+    y, desc = _run([3, 4096, 40], C2C, direction, 2, v, precision)
+    assert desc.count("transpose") == 2, desc
+    assert oracle.rel_l2(y, oracle.c2c(v, f, ndim=3)) <= oracle.tolerance(3 * 4096 * 40)
+    xr = rng.standard_normal((2, 2048, 100)).astype(np.float32)
+    y, desc = _run([2048, 100], R2C, direction, 2, xr, precision)
+    assert desc.count("transpose") == 2, desc  # the 2048-point axis over 51 bins
+    assert oracle.rel_l2(y, oracle.r2c(xr, f, ndim=2)) <= oracle.tolerance(2048 * 100)
+    xh = _rand_complex(rng, (2, 2048, 51))
+    y, desc = _run([2048, 100], C2R, direction, 2, xh, precision)
+    assert desc.count("transpose") == 2, desc
+    assert oracle.rel_l2(y, oracle.c2r(xh, 100, f, ndim=2)) <= oracle.tolerance(2048 * 100)
 
 
 def test_fp32_default_has_no_tensor_core_step(cuda):
