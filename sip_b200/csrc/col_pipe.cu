@@ -178,6 +178,13 @@ const void *col_pipe_kernel_fn(int n, int tpt, int tb, bool forward)
     return nullptr;
 }
 
+bool col_pipe_has_engine(int n)
+{
+    for (const ColPipeEntry &e : col_registry())
+        if (e.n == n) return true;
+    return false;
+}
+
 void col_pipe_kernel_fns(std::vector<const void *> &out)
 {
     for (const ColPipeEntry &e : col_registry()) {

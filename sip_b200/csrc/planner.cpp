@@ -386,14 +386,14 @@ struct Builder {
         p.steps.push_back(s);
     }
 
-    // Tensor-core form of a strided C2C axis [outer][n][inner] whose length has
-    // the warp-specialised row pipeline (1024, 2048, 4096 points): transpose the
-    // axis into contiguous rows in workspace, run the rows on the pipeline,
-    // transpose back.  Three HBM round trips instead of one, but the row
-    // pipeline keeps the tensor cores fed where the single-tile tensor-core
-    // kernel on column tiles is latency-bound (the reference runs its strided
-    // axes through explicit Transpose steps as well, core/fft/fft_api.cpp:527-697).
-    bool add_tc_strided(int64_t n, int64_t outer, int64_t inner, Buf src, Buf dst)
+    // A strided C2C axis [outer][n][inner] through transposes: transpose the axis
+    // into contiguous rows in workspace, run them on the row kernels (the
+    // tensor-core row pipeline in the split-precision forms), transpose back.
+    // Three HBM round trips instead of one, for axes whose column kernel is the
+    // slower (the single-tile tensor-core kernel is latency-bound; FP32 column
+    // tiles of long axes keep only 2-4 columns).  The reference runs its strided
+    // axes through explicit Transpose steps as well (core/fft/fft_api.cpp:527-697).
+    bool add_transposed_axis(int64_t n, int64_t outer, int64_t inner, Buf src, Buf dst)
     {
         const Buf a = free_ws({src, dst}), b = free_ws({src, dst, a});
         const size_t bytes = size_t(outer) * size_t(n) * size_t(inner) * sizeof(float2);
@@ -777,10 +777,24 @@ struct Builder {
             err = "strided axis of length " + std::to_string(n) + " has a prime factor above 13";
             return false;
         }
-        TcConfig tcc;
-        const int form = tc_form(n);
-        if ((form == 1 || form == 2) && !in_multipass && p.fft_type != 0x30 && tc_rows_config(static_cast<int>(n), tcc))
-            return add_tc_strided(n, outer, inner, src, dst);
+        // Through transposes: the tensor-core form of lengths with the row pipeline,
+        // and FP32 axes above 1024 points without a TMA column engine, whose column
+        // tiles shrink to 2-4 columns (16-32-byte row runs).  Measured, 2D C2C
+        // (column axis strided; us, column kernel -> transposes): 4096^2 x 2
+        // 539 -> 391, 8192 x 1024 x 4 690 -> 419, 3000 x 1024 x 8 605 -> 454,
+        // 6561 x 512 x 8 548 -> 459, 1500^2 x 12 446 -> 345; 1000^2 x 64 1146 -> 1330
+        // and 2048^2 x 8 244 -> 374 (TMA column engine) stay on column tiles.
+        // Vertical 1D plans keep their column tiles (complex32 data converts in
+        // the first and last tile steps).
+        if (!in_multipass && p.fft_type != 0x30) {
+            TcConfig tcc;
+            const int form = tc_form(n);
+            const bool tc = (form == 1 || form == 2) && tc_rows_config(static_cast<int>(n), tcc);
+            const bool slow_columns =
+                form == 0 && !p.vertical && n > 1024 && n <= kMaxStridedTile &&
+                !(col_pipe_has_engine(static_cast<int>(n)) && inner % 2 == 0);
+            if (tc || slow_columns) return add_transposed_axis(n, outer, inner, src, dst);
+        }
         TileCfg c;
         if (n > kMaxStridedTile || !choose_cfg(static_cast<int>(n), true, inner, c, err)) {
             // longer strided axes: multi-pass Stockham with 16-column tiles along the

@@ -72,6 +72,7 @@ const StaticKernel *find_static_kernel(int n, int io);
 // engines with 16 points per thread: n, threads per transform and columns per
 // tile must match an instantiation.
 const void *col_pipe_kernel_fn(int n, int tpt, int tb, bool forward);
+bool col_pipe_has_engine(int n);  // a TMA column engine exists for this length
 void col_pipe_kernel_fns(std::vector<const void *> &out);
 size_t col_pipe_smem(const TileDesc &d);
 // the step's input addressing and sizes fit the tensor map of the column kernel

@@ -117,7 +117,10 @@ def test_long_strided_axes(cuda, shape, typ):
     check(list(shape), typ, FWD, 2, seed=int(np.prod(shape)))
 
 
-SIZES_2D = [(1, 1), (3, 5), (32, 32), (64, 128), (100, 60), (2, 4096), (2048, 2048)]
+# (4096, 40), (1536, 33), (3000, 8): strided axes above 1024 points without a TMA column
+# engine, which run through transposes into rows
+SIZES_2D = [(1, 1), (3, 5), (32, 32), (64, 128), (100, 60), (2, 4096), (2048, 2048), (4096, 40), (1536, 33),
+            (3000, 8)]
 
 
 @pytest.mark.parametrize("xy", SIZES_2D)
@@ -128,7 +131,7 @@ def test_2d(cuda, xy, typ, fwd):
     check(list(xy), typ, fwd, batch, seed=xy[0] * 7 + xy[1])
 
 
-SIZES_3D = [(2, 3, 4), (8, 16, 32), (16, 16, 16), (5, 7, 30), (256, 256, 256)]
+SIZES_3D = [(2, 3, 4), (8, 16, 32), (16, 16, 16), (5, 7, 30), (256, 256, 256), (3, 4096, 8)]
 
 
 @pytest.mark.parametrize("xyz", SIZES_3D)
