@@ -229,6 +229,7 @@ struct BatchPlan {
     int *d_counters = nullptr;  // [0] = item counter, [1 + s] = tiles done of segment s
     size_t ws_bytes = 0;
     int grid = 1, block = kBatchBlock;
+    bool compact = false;  // every segment's radices are <= kCompactMaxRadix (three CTAs per SM)
     size_t smem = 0;
     std::vector<TablePtr> tables;
     int64_t in_elems = 0, out_elems = 0;
@@ -253,8 +254,13 @@ struct BatchPlan {
 
 namespace {
 
-std::string build_batch(BatchPlan &bp)
+std::string build_batch_with(BatchPlan &bp)
 {
+    bp.segs.clear();
+    bp.items.clear();
+    bp.seg_what.clear();
+    bp.tables.clear();
+    bp.smem = 0;
     int64_t in_off = 0, ws_off = 0;
     struct Pending {
         int seg;
@@ -279,6 +285,7 @@ std::string build_batch(BatchPlan &bp)
         p.row_smem = 48 * 1024;
         p.max_row_n = kBatchMaxRowN;
         p.max_maxe = kBatchMaxe;
+        p.max_radix = bp.compact ? kCompactMaxRadix : 16;
         std::string e = build_plan_1d(p);
         if (!e.empty()) return "length " + std::to_string(n) + ": " + e;
         const size_t ws0 = (p.ws_buf_bytes[0] + 255) / 256 * 256;
@@ -326,7 +333,7 @@ std::string build_batch(BatchPlan &bp)
     for (const Pending &pd : order)
         for (int t = 0; t < bp.segs[pd.seg].ntiles; t++) bp.items.push_back(make_int2(pd.seg, t));
     if (bp.items.size() > 0x7fffffff) return "too many tiles";
-    const int per_sm = kernel_blocks_per_sm(batch_kernel_fn(bp.forward), bp.block, bp.smem);
+    const int per_sm = kernel_blocks_per_sm(batch_kernel_fn(bp.forward, bp.compact), bp.block, bp.smem);
     if (per_sm <= 0) return "batch kernel does not fit on an SM";
     bp.grid = per_sm * sm_count(bp.device);
     size_t bytes = bp.segs.size() * sizeof(BatchSeg);
@@ -342,13 +349,27 @@ std::string build_batch(BatchPlan &bp)
     return std::string();
 }
 
+// The compact kernel (radices up to 10, three CTAs per SM) when every length
+// factors into them (16 and 12 split), else the kernel with every radix.
+std::string build_batch(BatchPlan &bp)
+{
+    bp.compact = true;
+    std::string e = build_batch_with(bp);
+    if (!e.empty() && e.find("needs a radix above") != std::string::npos) {
+        bp.compact = false;
+        e = build_batch_with(bp);
+    }
+    return e;
+}
+
 cudaError_t enqueue(BatchPlan &bp, const void *in, void *out, void *ws, cudaStream_t st)
 {
     cudaError_t e = cudaMemsetAsync(bp.d_counters, 0, (1 + bp.segs.size()) * sizeof(int), st);
     if (e != cudaSuccess) return e;
     BatchBufs bufs{{const_cast<void *>(in), out, ws, nullptr}};
     return launch_batch(bp.grid, bp.block, bp.smem, bp.d_segs, bp.d_items, static_cast<int>(bp.items.size()),
-                        bp.d_counters, bp.d_counters + 1, bufs, device_error_word(bp.device), bp.forward, st);
+                        bp.d_counters, bp.d_counters + 1, bufs, device_error_word(bp.device), bp.forward, bp.compact,
+                        st);
 }
 
 std::mutex g_batch_mu;
@@ -599,7 +620,7 @@ int64_t asdFftBatchDescribe(void *plan, char *buf, int64_t len)
     std::ostringstream o;
     o << "groups=" << bp->sizes.size() << " segments=" << bp->segs.size() << " items=" << bp->items.size()
       << " grid=" << bp->grid << " block=" << bp->block << " smem=" << bp->smem << " workspace=" << bp->ws_bytes
-      << "\n";
+      << " kernel=" << (bp->compact ? "compact radices <= 10" : "every radix") << "\n";
     for (size_t i = 0; i < bp->segs.size(); i++) {
         const auto &s = bp->segs[i];
         o << "  seg " << i << " n=" << s.d.n << " tiles=" << s.ntiles << " tb=" << s.d.tb << " tpt=" << s.d.tpt

@@ -30,12 +30,13 @@ namespace sipfft {
 // Register budget of one stage: NB butterflies of radix R per thread.
 template <int R, int MAXE>
 constexpr int nb_for() { return (MAXE + R - 1) / R; }
-template <int MAXE>
+template <int MAXE, bool COMPACT = false>
 constexpr int maxv_for()
 {
     constexpr int r[] = {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 16};
     int m = 0;
-    for (int x : r) m = m > ((MAXE + x - 1) / x) * x ? m : ((MAXE + x - 1) / x) * x;
+    for (int x : r)
+        if (!COMPACT || x <= kCompactMaxRadix) m = m > ((MAXE + x - 1) / x) * x ? m : ((MAXE + x - 1) / x) * x;
     return m;
 }
 
@@ -99,14 +100,18 @@ __device__ __forceinline__ void stage_write(const float2 *v, float2 *row, int n,
 }
 
 #define SIPFFT_RADIX_CASES(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(16)
+#define SIPFFT_COMPACT_RADIX_CASES(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
 
 // One register array is shared by all radices so that only one set of
 // butterfly values is live across each stage barrier.
 // kc >= 0: the tile's inter-pass twiddles (column kc) are still to be applied (first stage does it).
-template <int MAXE, bool FWD>
+// COMPACT: only radices up to kCompactMaxRadix are compiled (plans built with
+// Plan::max_radix = kCompactMaxRadix), which keeps the uneven-batch kernel at
+// three CTAs per SM.
+template <int MAXE, bool FWD, bool COMPACT = false>
 __device__ __forceinline__ void run_stages(float2 *row, const TileDesc &d, int lane, bool active, int64_t kc = -1)
 {
-    float2 v[maxv_for<MAXE>()];
+    float2 v[maxv_for<MAXE, COMPACT>()];
     int64_t toff = 0;  // offset of this stage's table in d.stw (stage 0 has none)
 #pragma unroll 1
     for (int s = 0; s < d.nstages; s++) {
@@ -114,21 +119,33 @@ __device__ __forceinline__ void run_stages(float2 *row, const TileDesc &d, int l
         const uint32_t nsm = d.ns_m[s];
         const float2 *tws = d.stw ? d.stw + toff : nullptr;
         if (s > 0) toff += int64_t(R - 1) * ns;
-        switch (R) {
 #define SIPFFT_READ(RR) \
     case RR: stage_read<RR, MAXE, FWD>(v, row, d.n, ns, nsm, ts, lane, d.tpt, active, d.tw, tws, d, s == 0 ? kc : -1); break;
-            SIPFFT_RADIX_CASES(SIPFFT_READ)
-#undef SIPFFT_READ
-            default: break;  // the planner only emits the radices above
-        }
-        __syncthreads();
-        switch (R) {
 #define SIPFFT_WRITE(RR) \
     case RR: stage_write<RR, MAXE>(v, row, d.n, ns, nsm, lane, d.tpt, active); break;
-            SIPFFT_RADIX_CASES(SIPFFT_WRITE)
-#undef SIPFFT_WRITE
-            default: break;
+        if constexpr (COMPACT) {
+            switch (R) {
+                SIPFFT_COMPACT_RADIX_CASES(SIPFFT_READ)
+                default: break;  // the planner only emits the radices above
+            }
+            __syncthreads();
+            switch (R) {
+                SIPFFT_COMPACT_RADIX_CASES(SIPFFT_WRITE)
+                default: break;
+            }
+        } else {
+            switch (R) {
+                SIPFFT_RADIX_CASES(SIPFFT_READ)
+                default: break;  // the planner only emits the radices above
+            }
+            __syncthreads();
+            switch (R) {
+                SIPFFT_RADIX_CASES(SIPFFT_WRITE)
+                default: break;
+            }
         }
+#undef SIPFFT_READ
+#undef SIPFFT_WRITE
         __syncthreads();
     }
 }
@@ -145,7 +162,7 @@ __device__ __forceinline__ void conj_tile(const TileDesc &d, float2 *sm, int ntr
 // their load and store phases do not depend on the direction)
 // loaded: the tile's input already sits in sm (copied by cp.async, inter-pass
 // twiddles not applied yet)
-template <int MAXE, bool FWD>
+template <int MAXE, bool FWD, bool COMPACT = false>
 __device__ __forceinline__ void process_tile(const TileDesc &d, const void *in, void *out, int64_t g, float2 *sm,
                                              bool flip = false, bool loaded = false)
 {
@@ -172,7 +189,7 @@ __device__ __forceinline__ void process_tile(const TileDesc &d, const void *in, 
         conj_tile(d, sm, ntr);
         __syncthreads();
     }
-    run_stages<MAXE, FWD>(sm + (thread_on ? l : 0) * d.pitch, d, lane, thread_on && l < ntr, kc);
+    run_stages<MAXE, FWD, COMPACT>(sm + (thread_on ? l : 0) * d.pitch, d, lane, thread_on && l < ntr, kc);
     if (flip) {
         conj_tile(d, sm, ntr);
         __syncthreads();
@@ -278,8 +295,10 @@ __device__ __forceinline__ void copy_desc(TileDesc *dst, const TileDesc &src)
     for (int i = threadIdx.x; i < static_cast<int>(sizeof(TileDesc) / 8); i += blockDim.x) d[i] = __ldg(s + i);
 }
 
-template <int MAXE, bool FWD>
-__global__ void __launch_bounds__(kBatchBlock, 2)
+// COMPACT (plans of radices <= kCompactMaxRadix): 80 registers, three CTAs per
+// SM; else every radix, two CTAs per SM.
+template <int MAXE, bool FWD, bool COMPACT>
+__global__ void __launch_bounds__(kBatchBlock, COMPACT ? 3 : 2)
     batch_fft_kernel(const BatchSeg *__restrict__ segs, const int2 *__restrict__ items, int nitems, int *counter,
                      int *done, BatchBufs bufs, int *err, int64_t span)
 {
@@ -346,7 +365,7 @@ __global__ void __launch_bounds__(kBatchBlock, 2)
         if (ok) {
             // a Bluestein segment runs its convolution FFTs in both directions; the
             // other direction is conj(DFT(conj(y))) around this kernel's stages
-            process_tile<MAXE, FWD>(s_desc[i & 1], in, out, it.y, cur, sg.fwd != (FWD ? 1 : 0), pref);
+            process_tile<MAXE, FWD, COMPACT>(s_desc[i & 1], in, out, it.y, cur, sg.fwd != (FWD ? 1 : 0), pref);
             if (tid == 0) {
                 __threadfence();
                 atomicAdd(done + it.x, 1);
@@ -450,8 +469,10 @@ void tile_kernel_fns(std::vector<const void *> &out)
     out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<16, false>));
     out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<32, true>));
     out.push_back(reinterpret_cast<const void *>(tile_fft_kernel<32, false>));
-    out.push_back(batch_kernel_fn(true));
-    out.push_back(batch_kernel_fn(false));
+    for (int c = 0; c < 2; c++) {
+        out.push_back(batch_kernel_fn(true, c != 0));
+        out.push_back(batch_kernel_fn(false, c != 0));
+    }
     for (int maxe : {8, 16, 32})
         for (int f = 0; f < 2; f++) out.push_back(tile_db_kernel_fn(maxe, f != 0));
 }
@@ -490,16 +511,20 @@ cudaError_t launch_tile(const TileDesc &d, int maxe, bool forward, int grid, cud
     return forward ? launch_one<32, true>(d, grid, block, smem, st) : launch_one<32, false>(d, grid, block, smem, st);
 }
 
-const void *batch_kernel_fn(bool forward)
+const void *batch_kernel_fn(bool forward, bool compact)
 {
-    return forward ? reinterpret_cast<const void *>(batch_fft_kernel<kBatchMaxe, true>)
-                   : reinterpret_cast<const void *>(batch_fft_kernel<kBatchMaxe, false>);
+    if (compact)
+        return forward ? reinterpret_cast<const void *>(batch_fft_kernel<kBatchMaxe, true, true>)
+                       : reinterpret_cast<const void *>(batch_fft_kernel<kBatchMaxe, false, true>);
+    return forward ? reinterpret_cast<const void *>(batch_fft_kernel<kBatchMaxe, true, false>)
+                   : reinterpret_cast<const void *>(batch_fft_kernel<kBatchMaxe, false, false>);
 }
 
 cudaError_t launch_batch(int grid, int block, size_t smem, const BatchSeg *segs, const int2 *items, int nitems,
-                         int *counter, int *done, const BatchBufs &bufs, int *err, bool forward, cudaStream_t st)
+                         int *counter, int *done, const BatchBufs &bufs, int *err, bool forward, bool compact,
+                         cudaStream_t st)
 {
-    const void *fn = batch_kernel_fn(forward);
+    const void *fn = batch_kernel_fn(forward, compact);
     BatchBufs b = bufs;
     int64_t span = static_cast<int64_t>(smem / 2 / sizeof(float2));  // float2 per buffer
     void *args[] = {&segs, &items, &nitems, &counter, &done, &b, &err, &span};

@@ -171,6 +171,29 @@ bool split_passes(int64_t n, int parts, std::vector<int> &out)
     return true;
 }
 
+// Splits radices above max_r into supported pairs (16 = 4 x 4, 12 = 4 x 3);
+// false when a prime radix (11, 13) is above it.
+bool limit_radices(std::vector<int> &radices, int max_r)
+{
+    if (max_r >= 16) return true;
+    std::vector<int> out;
+    for (int r : radices) {
+        if (r <= max_r) {
+            out.push_back(r);
+        } else if (r == 16 && max_r >= 4) {
+            out.push_back(4);
+            out.push_back(4);
+        } else if (r == 12 && max_r >= 4) {
+            out.push_back(4);
+            out.push_back(3);
+        } else {
+            return false;
+        }
+    }
+    radices = out;
+    return static_cast<int>(radices.size()) <= kMaxStages;
+}
+
 struct Builder {
     Plan &p;
     bool fwd;
@@ -275,6 +298,10 @@ struct Builder {
             radices = tc.radices;
             maxe_override = tc.maxe;
             if (tc.row_threads > 0 && tc.row_threads <= p.row_threads) row_threads = tc.row_threads;
+        }
+        if (!limit_radices(radices, p.max_radix)) {
+            err = "length " + std::to_string(n) + " needs a radix above " + std::to_string(p.max_radix);
+            return false;
         }
         TileCfg c;
         if (!choose_cfg(n, column, n_cols, c, err, maxe_override, row_threads, p.row_smem, p.max_maxe,

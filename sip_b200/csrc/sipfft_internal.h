@@ -48,9 +48,13 @@ void static_kernel_fns(std::vector<const void *> &out);
 constexpr int kBatchBlock = 256;
 constexpr int kBatchMaxe = 16;
 constexpr int64_t kBatchMaxRowN = 4096;
-const void *batch_kernel_fn(bool forward);
+// radices of the compact uneven-batch kernel (larger ones are split: 16 = 4 x 4,
+// 12 = 4 x 3; lengths with a factor 11 or 13 use the kernel with every radix)
+constexpr int kCompactMaxRadix = 10;
+const void *batch_kernel_fn(bool forward, bool compact);
 cudaError_t launch_batch(int grid, int block, size_t smem, const BatchSeg *segs, const int2 *items, int nitems,
-                         int *counter, int *done, const BatchBufs &bufs, int *err, bool forward, cudaStream_t st);
+                         int *counter, int *done, const BatchBufs &bufs, int *err, bool forward, bool compact,
+                         cudaStream_t st);
 cudaError_t launch_kernel_fn(const void *fn, const TileDesc &d, int grid, size_t smem, int *err, cudaStream_t st);
 // Launch with programmatic stream serialization (the kernel calls pdl_enter()
 // before its first global access).
@@ -241,6 +245,7 @@ struct Plan {
     int row_smem = 64 * 1024;  // shared memory per CTA the row tiles stay under
     int64_t max_row_n = 1 << 30;  // C2C rows longer than this take the multi-pass path
     int max_maxe = 32;            // largest points per thread a tile may use (tuned choices above are ignored)
+    int max_radix = 16;           // largest radix a tile may use (16 and 12 split below it)
     // inverse STFT plan (asdFftIstftMakePlan): one column C2C step into workspace
     // slot 0 ([channel][frame][n_fft]), then the overlap-add kernel
     bool istft = false;

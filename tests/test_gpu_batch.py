@@ -49,6 +49,24 @@ def test_uneven_small(cuda, use_graph, direction):
     plan.close()
 
 
+@pytest.mark.parametrize("direction", [fft.ASCEND_FFT_FORWARD, fft.ASCEND_FFT_INVERSE])
+def test_compact_and_full_radix_kernels(cuda, direction):
+    """Lengths whose radices fit 2..10 (16 and 12 split) run on the compact batch
+    kernel (three CTAs per SM); a length with a factor 11 or 13 selects the kernel
+    with every radix.  Both against the oracle, multi-pass lengths included."""
+    fwd = direction == fft.ASCEND_FFT_FORWARD
+    compact = [(48, 7), (144, 5), (240, 3), (4096, 2), (3 * 2 ** 12, 2), (52920, 1), (65536, 1)]
+    plan, x, outs = _run(compact, direction, seed=5)
+    assert "kernel=compact" in plan.describe(), plan.describe()
+    _check(plan, x, outs[0], fwd)
+    plan.close()
+    full = compact[:3] + [(11 * 64, 4), (13 * 13 * 16, 2)]
+    plan, x, outs = _run(full, direction, seed=6)
+    assert "kernel=every radix" in plan.describe(), plan.describe()
+    _check(plan, x, outs[0], fwd)
+    plan.close()
+
+
 def test_uneven_workload_subset(cuda):
     """A slice of the seeded 20 000-transform set (lengths 64..65536, Zipf batches)."""
     groups = workloads.uneven_batch_set(total=2000, seed=7)
