@@ -100,29 +100,31 @@ __device__ __forceinline__ void r2c_post_row(const float2 *work, float2 *y, int 
     }
 }
 
-template <int MAXE>
+// COMPACT: radices up to kCompactRadix only, CTAs of at most 256 threads,
+// three per SM (80 registers); else every radix, up to 512 threads.
+template <int MAXE, bool COMPACT = false>
 struct RuntimeEngine {
     static constexpr bool kPingPong = false;
-    static constexpr int kMaxThreads = 512;
-    static constexpr int kMinBlocks = 1;
+    static constexpr int kMaxThreads = COMPACT ? 256 : 512;
+    static constexpr int kMinBlocks = COMPACT ? 3 : 1;
     template <bool FWD, class Src0, class DstL>
     __device__ __forceinline__ static void run(const TileDesc &d, float2 *work, const Src0 &src0, const DstL &dstL,
                                                bool dst_in_place, int lane, bool active, float2 * = nullptr)
     {
-        run_fft<MAXE, FWD>(d, work, src0, true, dstL, dst_in_place, lane, active);
+        run_fft<MAXE, FWD, COMPACT>(d, work, src0, true, dstL, dst_in_place, lane, active);
     }
     template <bool FWD, class DstL>
     __device__ __forceinline__ static void run_c2r(const TileDesc &d, float2 *work, const float2 *x, const DstL &dstL,
                                                    int lane, bool active, float2 * = nullptr)
     {
-        run_fft<MAXE, FWD>(d, work, C2RPre<FWD>{x, d.n, d.tw}, true, dstL, false, lane, active);
+        run_fft<MAXE, FWD, COMPACT>(d, work, C2RPre<FWD>{x, d.n, d.tw}, true, dstL, false, lane, active);
     }
     // R2C: packed FFT into the work row, then the post-twiddle pass to HBM
     template <bool FWD, class Src0>
     __device__ __forceinline__ static void run_r2c(const TileDesc &d, float2 *work, const Src0 &src0, float2 *y,
                                                    int lane, bool active, float2 * = nullptr)
     {
-        run_fft<MAXE, FWD>(d, work, src0, true, SmemRow{work}, true, lane, active);
+        run_fft<MAXE, FWD, COMPACT>(d, work, src0, true, SmemRow{work}, true, lane, active);
         __syncthreads();
         if (active) r2c_post_row<FWD>(work, y, d.n, lane, d.tpt, d.tw);
     }

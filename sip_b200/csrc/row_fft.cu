@@ -22,10 +22,23 @@ const void *row_fn_io32(bool forward, int io)
     return forward ? runtime_row_kernel_32_fwd(io) : runtime_row_kernel_32_inv(io);
 }
 
+// the compact engine when the tile's radices are all <= kCompactRadix and its
+// CTA has at most 256 threads
+bool compact_ok(const TileDesc &d)
+{
+    if (d.tb * d.tpt > 256) return false;
+    for (int s = 0; s < d.nstages; s++)
+        if (d.radix[s] > kCompactRadix) return false;
+    return true;
+}
+
 const void *pick(const TileDesc &d, int maxe, bool forward)
 {
     if (maxe <= 8) return row_fn_io8(forward, d.io);
-    if (maxe <= 16) return row_fn_io16(forward, d.io);
+    if (maxe <= 16) {
+        if (compact_ok(d)) return forward ? runtime_row_kernel_16c_fwd(d.io) : runtime_row_kernel_16c_inv(d.io);
+        return row_fn_io16(forward, d.io);
+    }
     return row_fn_io32(forward, d.io);
 }
 
@@ -90,6 +103,7 @@ void row_kernel_fns(std::vector<const void *> &out)
             out.push_back(row_fn_io8(f, io));
             out.push_back(row_fn_io16(f, io));
             out.push_back(row_fn_io32(f, io));
+            out.push_back(f ? runtime_row_kernel_16c_fwd(io) : runtime_row_kernel_16c_inv(io));
         }
     }
 }

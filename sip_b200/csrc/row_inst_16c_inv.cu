@@ -1,0 +1,9 @@
+// Runtime-radix row kernels of the compact radix set (2..10), at most 16 points
+// per thread, INVERSE direction.
+#include "row_fft_inst.cuh"
+
+namespace sipfft {
+
+const void *runtime_row_kernel_16c_inv(int io) { return runtime_row_kernel<16, false, true>(io); }
+
+}  // namespace sipfft

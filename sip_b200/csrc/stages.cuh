@@ -27,12 +27,17 @@ __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
 template <int R, int MAXE>
 constexpr int nb_for() { return (MAXE + R - 1) / R; }
 
-template <int MAXE>
+// Largest radix of the compact engines (compiled without the radix 11-16
+// codelets, so that they fit three CTAs per SM); the planner splits 16 and 12.
+constexpr int kCompactRadix = 10;
+
+template <int MAXE, bool COMPACT = false>
 constexpr int maxv_for()
 {
     constexpr int r[] = {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 16};
     int m = 0;
-    for (int x : r) m = m > ((MAXE + x - 1) / x) * x ? m : ((MAXE + x - 1) / x) * x;
+    for (int x : r)
+        if (!COMPACT || x <= kCompactRadix) m = m > ((MAXE + x - 1) / x) * x ? m : ((MAXE + x - 1) / x) * x;
     return m;
 }
 
@@ -99,31 +104,46 @@ __device__ __forceinline__ void stage_scatter(const float2 *v, const Dst &dst, i
 }
 
 #define SIPFFT_RADIX_CASES(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(16)
+#define SIPFFT_COMPACT_RADIX_CASES(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
 
-template <int MAXE, bool FWD, class Src>
+template <int MAXE, bool FWD, bool COMPACT, class Src>
 __device__ __forceinline__ void gather_any(int R, float2 *v, const Src &src, int n, int ns, uint32_t nsm, int ts,
                                            int lane, int tpt, bool active, const float2 *tw, const float2 *tws)
 {
-    switch (R) {
 #define SIPFFT_G(RR) \
     case RR: stage_gather<RR, MAXE, FWD>(v, src, n, ns, nsm, ts, lane, tpt, active, tw, tws); break;
-        SIPFFT_RADIX_CASES(SIPFFT_G)
-#undef SIPFFT_G
-        default: break;
+    if constexpr (COMPACT) {
+        switch (R) {
+            SIPFFT_COMPACT_RADIX_CASES(SIPFFT_G)
+            default: break;
+        }
+    } else {
+        switch (R) {
+            SIPFFT_RADIX_CASES(SIPFFT_G)
+            default: break;
+        }
     }
+#undef SIPFFT_G
 }
 
-template <int MAXE, class Dst>
+template <int MAXE, bool COMPACT, class Dst>
 __device__ __forceinline__ void scatter_any(int R, const float2 *v, const Dst &dst, int n, int ns, uint32_t nsm,
                                             int lane, int tpt, bool active)
 {
-    switch (R) {
 #define SIPFFT_S(RR) \
     case RR: stage_scatter<RR, MAXE>(v, dst, n, ns, nsm, lane, tpt, active); break;
-        SIPFFT_RADIX_CASES(SIPFFT_S)
-#undef SIPFFT_S
-        default: break;
+    if constexpr (COMPACT) {
+        switch (R) {
+            SIPFFT_COMPACT_RADIX_CASES(SIPFFT_S)
+            default: break;
+        }
+    } else {
+        switch (R) {
+            SIPFFT_RADIX_CASES(SIPFFT_S)
+            default: break;
+        }
     }
+#undef SIPFFT_S
 }
 
 // Full FFT of one transform per thread group.
@@ -131,11 +151,11 @@ __device__ __forceinline__ void scatter_any(int R, const float2 *v, const Dst &d
 //   dstL     — where the last stage writes (may be the work row: dstL_in_place)
 // Every other stage runs in place in the padded work row.  On return the
 // caller must barrier before reusing `work` if dstL wrote into it.
-template <int MAXE, bool FWD, class Src0, class DstL>
+template <int MAXE, bool FWD, bool COMPACT = false, class Src0, class DstL>
 __device__ __forceinline__ void run_fft(const TileDesc &d, float2 *work, const Src0 &src0, bool src0_in_place,
                                         const DstL &dstL, bool dstL_in_place, int lane, bool active)
 {
-    float2 v[maxv_for<MAXE>()];
+    float2 v[maxv_for<MAXE, COMPACT>()];
     const int S = d.nstages;
     const int n = d.n;
     const SmemRow w{work};
@@ -147,26 +167,26 @@ __device__ __forceinline__ void run_fft(const TileDesc &d, float2 *work, const S
     // stage 0 (no twiddles); stage s >= 1 reads d.stw + toff when the plan has stage tables
     int64_t toff = 0;
     auto tws = [&](int s) -> const float2 * { return d.stw ? d.stw + toff : nullptr; };
-    gather_any<MAXE, FWD>(d.radix[0], v, src0, n, d.ns[0], d.ns_m[0], d.tstep[0], lane, d.tpt, active, d.tw, nullptr);
+    gather_any<MAXE, FWD, COMPACT>(d.radix[0], v, src0, n, d.ns[0], d.ns_m[0], d.tstep[0], lane, d.tpt, active, d.tw, nullptr);
     if (src0_in_place || (S == 1 && dstL_in_place)) __syncthreads();
     if (S == 1) {
-        scatter_any<MAXE>(d.radix[0], v, dstL, n, d.ns[0], d.ns_m[0], lane, d.tpt, active);
+        scatter_any<MAXE, COMPACT>(d.radix[0], v, dstL, n, d.ns[0], d.ns_m[0], lane, d.tpt, active);
         return;
     }
-    scatter_any<MAXE>(d.radix[0], v, w, n, d.ns[0], d.ns_m[0], lane, d.tpt, active);
+    scatter_any<MAXE, COMPACT>(d.radix[0], v, w, n, d.ns[0], d.ns_m[0], lane, d.tpt, active);
     __syncthreads();
 #pragma unroll 1
     for (int s = 1; s < S - 1; s++) {
-        gather_any<MAXE, FWD>(d.radix[s], v, w, n, d.ns[s], d.ns_m[s], d.tstep[s], lane, d.tpt, active, d.tw, tws(s));
+        gather_any<MAXE, FWD, COMPACT>(d.radix[s], v, w, n, d.ns[s], d.ns_m[s], d.tstep[s], lane, d.tpt, active, d.tw, tws(s));
         toff += int64_t(d.radix[s] - 1) * d.ns[s];
         __syncthreads();
-        scatter_any<MAXE>(d.radix[s], v, w, n, d.ns[s], d.ns_m[s], lane, d.tpt, active);
+        scatter_any<MAXE, COMPACT>(d.radix[s], v, w, n, d.ns[s], d.ns_m[s], lane, d.tpt, active);
         __syncthreads();
     }
-    gather_any<MAXE, FWD>(d.radix[S - 1], v, w, n, d.ns[S - 1], d.ns_m[S - 1], d.tstep[S - 1], lane, d.tpt, active, d.tw,
+    gather_any<MAXE, FWD, COMPACT>(d.radix[S - 1], v, w, n, d.ns[S - 1], d.ns_m[S - 1], d.tstep[S - 1], lane, d.tpt, active, d.tw,
                           tws(S - 1));
     if (dstL_in_place) __syncthreads();
-    scatter_any<MAXE>(d.radix[S - 1], v, dstL, n, d.ns[S - 1], d.ns_m[S - 1], lane, d.tpt, active);
+    scatter_any<MAXE, COMPACT>(d.radix[S - 1], v, dstL, n, d.ns[S - 1], d.ns_m[S - 1], lane, d.tpt, active);
 }
 
 }  // namespace sipfft
