@@ -97,6 +97,16 @@ __device__ __forceinline__ void pdl_enter()
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// The same two steps apart: a kernel that lets the next one launch only from
+// its last tile keeps the next kernel's waiting CTAs off its SMs until its
+// tail (used by the row kernel, whose compact-engine CTAs leave room beside
+// them for another kernel's CTAs).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Output element store that allocates no L1 line: streamed FFT output would
 // otherwise evict the twiddle tables that the next tiles read from L1.
 __device__ __forceinline__ void st_stream(float2 *p, float2 v)

@@ -134,7 +134,7 @@ template <class Engine, bool FWD, int IO>
 __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
     pipelined_rows_kernel(const __grid_constant__ TileDesc d, int *err)
 {
-    pdl_enter();
+    pdl_wait();
     extern __shared__ __align__(128) unsigned char smraw[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smraw);
     const int64_t buf_f2 = d.g_ns;  // per-buffer float2 count (planner-computed, even)
@@ -187,6 +187,7 @@ __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
         // tile (on whatever the buffer holds: every access stays in bounds), so
         // that every thread reaches the same barriers; the CTA leaves together
         // at the end of the iteration.
+        if (tn >= d.num_tiles) pdl_launch_dependents();  // this CTA's last tile (a CTA without tiles: at exit)
         const bool timed_out = !mbar_wait_bounded(&bars[b], (i >> 1) & 1);
         if (timed_out) atomicExch(err, 1);
         const int rows = tile_rows(t);
