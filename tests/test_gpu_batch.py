@@ -55,7 +55,9 @@ def test_compact_and_full_radix_kernels(cuda, direction):
     kernel (three CTAs per SM); a length with a factor 11 or 13 selects the kernel
     with every radix.  Both against the oracle, multi-pass lengths included."""
     fwd = direction == fft.ASCEND_FFT_FORWARD
-    compact = [(48, 7), (144, 5), (240, 3), (4096, 2), (3 * 2 ** 12, 2), (52920, 1), (65536, 1)]
+    # 17 and 1021 are Bluestein lengths: power-of-two convolutions, radix 16 split into 4 x 4
+    compact = [(17, 11), (48, 7), (144, 5), (240, 3), (1021, 3), (4096, 2), (3 * 2 ** 12, 2), (52920, 1),
+               (65536, 1)]
     plan, x, outs = _run(compact, direction, seed=5)
     assert "kernel=compact" in plan.describe(), plan.describe()
     _check(plan, x, outs[0], fwd)
