@@ -17,6 +17,11 @@
 namespace sipfft {
 
 constexpr int kMaxStages = 16;
+// Largest radix of the compact runtime-radix engines (compiled without the
+// radix 11-16 codelets so that they fit three CTAs per SM; a plan for them
+// splits 16 = 4 x 4 and 12 = 4 x 3, and lengths with a factor 11 or 13 use the
+// engines with every radix).
+constexpr int kCompactMaxRadix = 10;
 
 enum IoKind : int {
     IO_C2C = 0,         // complex in, complex out

@@ -100,7 +100,7 @@ __device__ __forceinline__ void r2c_post_row(const float2 *work, float2 *y, int 
     }
 }
 
-// COMPACT: radices up to kCompactRadix only, CTAs of at most 256 threads,
+// COMPACT: radices up to kCompactMaxRadix only, CTAs of at most 256 threads,
 // three per SM (80 registers); else every radix, up to 512 threads.
 template <int MAXE, bool COMPACT = false>
 struct RuntimeEngine {

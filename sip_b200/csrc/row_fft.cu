@@ -22,13 +22,13 @@ const void *row_fn_io32(bool forward, int io)
     return forward ? runtime_row_kernel_32_fwd(io) : runtime_row_kernel_32_inv(io);
 }
 
-// the compact engine when the tile's radices are all <= kCompactRadix and its
+// the compact engine when the tile's radices are all <= kCompactMaxRadix and its
 // CTA has at most 256 threads
 bool compact_ok(const TileDesc &d)
 {
     if (d.tb * d.tpt > 256) return false;
     for (int s = 0; s < d.nstages; s++)
-        if (d.radix[s] > kCompactRadix) return false;
+        if (d.radix[s] > kCompactMaxRadix) return false;
     return true;
 }
 

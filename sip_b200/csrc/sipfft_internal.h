@@ -48,9 +48,6 @@ void static_kernel_fns(std::vector<const void *> &out);
 constexpr int kBatchBlock = 256;
 constexpr int kBatchMaxe = 16;
 constexpr int64_t kBatchMaxRowN = 4096;
-// radices of the compact uneven-batch kernel (larger ones are split: 16 = 4 x 4,
-// 12 = 4 x 3; lengths with a factor 11 or 13 use the kernel with every radix)
-constexpr int kCompactMaxRadix = 10;
 const void *batch_kernel_fn(bool forward, bool compact);
 cudaError_t launch_batch(int grid, int block, size_t smem, const BatchSeg *segs, const int2 *items, int nitems,
                          int *counter, int *done, const BatchBufs &bufs, int *err, bool forward, bool compact,

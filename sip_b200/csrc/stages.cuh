@@ -27,17 +27,13 @@ __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
 template <int R, int MAXE>
 constexpr int nb_for() { return (MAXE + R - 1) / R; }
 
-// Largest radix of the compact engines (compiled without the radix 11-16
-// codelets, so that they fit three CTAs per SM); the planner splits 16 and 12.
-constexpr int kCompactRadix = 10;
-
 template <int MAXE, bool COMPACT = false>
 constexpr int maxv_for()
 {
     constexpr int r[] = {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 16};
     int m = 0;
     for (int x : r)
-        if (!COMPACT || x <= kCompactRadix) m = m > ((MAXE + x - 1) / x) * x ? m : ((MAXE + x - 1) / x) * x;
+        if (!COMPACT || x <= kCompactMaxRadix) m = m > ((MAXE + x - 1) / x) * x ? m : ((MAXE + x - 1) / x) * x;
     return m;
 }
 
