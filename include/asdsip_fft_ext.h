@@ -37,9 +37,12 @@ ASDSIP_API int32_t asdFftPlanLaunchCount(void *handle);
  *         with asdFftTuneCacheLoad) measured fastest on this GPU; FP32 for lengths it has not timed.
  * Tensor-core stages exist for transform lengths 256, 1024, 2048 and 4096 of a C2C axis (and 512, 2048,
  * 4096 and 8192 for R2C / C2R, whose packed inner transform has half the length); every other step keeps the FP32
- * kernels, which asdFftDescribePlan shows.  May be called before or after MakePlan*: an initialised
- * plan is rebuilt (the workspace size does not change).  Returns ACL_ERROR_INVALID_PARAM for an unknown
- * handle or mode. */
+ * kernels, which asdFftDescribePlan shows.  Strided axes of 1024, 2048 and 4096 points run their
+ * tensor-core stages as rows between two transposes, which needs workspace for two copies of the data.
+ * May be called before or after MakePlan*: an initialised plan is rebuilt; when the rebuilt plan needs
+ * more workspace than before, the workspace set earlier is dropped (exec then returns the missing-
+ * workspace error) and asdFftGetWorkspaceSize reports the new size for asdFftSetWorkspace.  Returns
+ * ACL_ERROR_INVALID_PARAM for an unknown handle or mode. */
 ASDSIP_API int32_t asdFftSetPrecision(void *handle, int32_t mode);
 
 /* ---- uneven batches: many 1D C2C groups (length sizes[i], count batches[i]) stored back to back,

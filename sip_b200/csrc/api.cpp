@@ -672,9 +672,11 @@ int32_t asdFftSetPrecision(void *handle, int32_t mode)
                                                                     : sipfft::build_plan_3d;
     const AspbStatus st = finish_plan(*p, builder, "asdFftSetPrecision");
     if (st == AsdSip::ACL_SUCCESS && p->ws_bytes > ws) {
-        p->initialized = false;
-        log_error("asdFftSetPrecision", "rebuilt plan needs a larger workspace");
-        return AsdSip::ACL_ERROR_INTERNAL_ERROR;
+        // the rebuilt plan needs more workspace (a strided axis through transposes):
+        // the old buffer is too small, so it is dropped and exec refuses to run
+        // (missing workspace) until the caller sets one of the new size
+        p->workspace = nullptr;
+        log_error("asdFftSetPrecision", "rebuilt plan needs a larger workspace: query and set it again");
     }
     return st;
 }

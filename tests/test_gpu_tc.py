@@ -195,6 +195,36 @@ def test_fp32_default_has_no_tensor_core_step(cuda):
     assert oracle.rel_l2(y, oracle.c2c(x, True)) <= oracle.tolerance(1024)
 
 
+def test_set_precision_after_plan_grows_workspace(cuda):
+    """A 2D plan made in FP32 needs no workspace; switched to a tensor-core form its
+    1024-point strided axis runs between two transposes and needs workspace: the
+    call succeeds, exec refuses until a workspace of the new size is set, then runs."""
+    import torch
+
+    plan = fft.FftPlan([1024, 64], C2C, FWD, 2)
+    try:
+        lib = fft.load_library()
+        st, ws0 = fft.asdFftGetWorkspaceSize(plan.handle)
+        assert st == fft.ACL_SUCCESS and ws0 == 0
+        assert lib.asdFftSetPrecision(plan.handle, fft.PRECISION_BF16X3) == fft.ACL_SUCCESS
+        st, ws1 = fft.asdFftGetWorkspaceSize(plan.handle)
+        assert st == fft.ACL_SUCCESS and ws1 >= 2 * 2 * 1024 * 64 * 8, ws1
+        rng = np.random.default_rng(12)
+        x = _rand_complex(rng, (2, 1024, 64))
+        xin = torch.from_numpy(x).cuda()
+        out = torch.empty_like(xin)
+        with pytest.raises(fft.FftError):
+            plan(xin, out)
+        wsp = torch.empty(ws1, dtype=torch.uint8, device="cuda")
+        assert fft.asdFftSetWorkspace(plan.handle, wsp.data_ptr()) == fft.ACL_SUCCESS
+        plan(xin, out)
+        torch.cuda.synchronize()
+        assert "transpose" in plan.describe()
+        assert oracle.rel_l2(out.cpu().numpy(), oracle.c2c(x, True, ndim=2)) <= oracle.tolerance(1024 * 64)
+    finally:
+        plan.close()
+
+
 def test_set_precision_after_plan_rebuilds(cuda):
     import torch
 
