@@ -9,6 +9,8 @@
 // long as the bytes in flight stay within the workspace budget; it copies the
 // inputs in (one cudaMemcpyAsync per request), runs the plan re-targeted to
 // the batch's row count, copies each request's rows out and records an event.
+// Requests in device memory of 8 MB or more skip the staging copies: the plan
+// runs on their own buffers, on the lane's stream and workspace.
 // Batches on different lanes run concurrently, so requests that arrive while
 // others are on the GPU are admitted as soon as a lane and budget free up.
 // Per-request latency is measured from submission to the host observing the
@@ -65,6 +67,8 @@ struct Lane {
 };
 
 int64_t in_bytes(const Req &r) { return r.type == 0x12 ? r.rows * r.n * 4 : r.rows * r.n * 8; }
+// device-memory requests at least this large run on their own buffers
+constexpr int64_t kDirectBytes = int64_t(8) << 20;
 int64_t out_bytes(const Req &r) { return r.type == 0x12 ? r.rows * (r.n / 2 + 1) * 8 : r.rows * r.n * 8; }
 
 }  // namespace
@@ -258,29 +262,45 @@ private:
             p = plan_for(h.type, h.dir, h.n);
         }
         if (!p) return false;
+        if (!grow(l.d_ws, l.bytes_ws, std::max<size_t>(p->ws_bytes, 256))) return false;
+        // Requests in device memory of at least kDirectBytes run the plan on their
+        // own buffers (a staged copy in and out would double their HBM traffic);
+        // smaller ones, and every request in host memory, are copied into the
+        // lane's staging buffers and run as one batch.
+        std::vector<const Req *> staged;
         int64_t rows = 0;
-        for (const Req &r : l.batch) rows += r.rows;
-        std::vector<Step> steps;
-        if (!scale_steps_to_rows(*p, rows, steps)) return false;
-        const size_t ib = static_cast<size_t>(in_bytes(h) / h.rows * max_rows_);
-        const size_t ob = static_cast<size_t>(out_bytes(h) / h.rows * max_rows_);
-        if (!grow(l.d_in, l.bytes_in, ib) || !grow(l.d_out, l.bytes_out, ob) ||
-            !grow(l.d_ws, l.bytes_ws, std::max<size_t>(p->ws_bytes, 256)))
-            return false;
-        const cudaMemcpyKind kin = device_io_ ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-        const cudaMemcpyKind kout = device_io_ ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-        size_t off = 0;
         for (const Req &r : l.batch) {
-            const size_t b = static_cast<size_t>(in_bytes(r));
-            if (cudaMemcpyAsync(l.d_in + off, r.in, b, kin, l.stream) != cudaSuccess) return false;
-            off += b;
+            const bool aligned = (reinterpret_cast<uintptr_t>(r.in) | reinterpret_cast<uintptr_t>(r.out)) % 16 == 0;
+            if (device_io_ && aligned && in_bytes(r) >= kDirectBytes) {
+                std::vector<Step> steps;
+                if (!scale_steps_to_rows(*p, r.rows, steps)) return false;
+                if (execute_steps(*p, steps, r.in, r.out, l.d_ws, l.stream) != cudaSuccess) return false;
+            } else {
+                staged.push_back(&r);
+                rows += r.rows;
+            }
         }
-        if (execute_steps(*p, steps, l.d_in, l.d_out, l.d_ws, l.stream) != cudaSuccess) return false;
-        off = 0;
-        for (const Req &r : l.batch) {
-            const size_t b = static_cast<size_t>(out_bytes(r));
-            if (cudaMemcpyAsync(r.out, l.d_out + off, b, kout, l.stream) != cudaSuccess) return false;
-            off += b;
+        if (!staged.empty()) {
+            std::vector<Step> steps;
+            if (!scale_steps_to_rows(*p, rows, steps)) return false;
+            const size_t ib = static_cast<size_t>(in_bytes(h) / h.rows * max_rows_);
+            const size_t ob = static_cast<size_t>(out_bytes(h) / h.rows * max_rows_);
+            if (!grow(l.d_in, l.bytes_in, ib) || !grow(l.d_out, l.bytes_out, ob)) return false;
+            const cudaMemcpyKind kin = device_io_ ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+            const cudaMemcpyKind kout = device_io_ ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+            size_t off = 0;
+            for (const Req *r : staged) {
+                const size_t b = static_cast<size_t>(in_bytes(*r));
+                if (cudaMemcpyAsync(l.d_in + off, r->in, b, kin, l.stream) != cudaSuccess) return false;
+                off += b;
+            }
+            if (execute_steps(*p, steps, l.d_in, l.d_out, l.d_ws, l.stream) != cudaSuccess) return false;
+            off = 0;
+            for (const Req *r : staged) {
+                const size_t b = static_cast<size_t>(out_bytes(*r));
+                if (cudaMemcpyAsync(r->out, l.d_out + off, b, kout, l.stream) != cudaSuccess) return false;
+                off += b;
+            }
         }
         return cudaEventRecord(l.done, l.stream) == cudaSuccess;
     }
