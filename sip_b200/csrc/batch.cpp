@@ -92,7 +92,8 @@ bool parse_line(const std::string &line, std::string &gpu, int64_t &n, TuneChoic
     };
     gpu = field("gpu");
     const std::string ns = field("n"), rs = field("radices"), ms = field("maxe"), us = field("us");
-    if (gpu.empty() || ns.empty() || rs.empty() || field("type") != "c2c") return false;
+    if (gpu.empty() || ns.empty() || line.find("\"radices\":") == std::string::npos || field("type") != "c2c")
+        return false;
     n = std::atoll(ns.c_str());
     c.radices.clear();
     std::stringstream ss(rs);
@@ -104,7 +105,8 @@ bool parse_line(const std::string &line, std::string &gpu, int64_t &n, TuneChoic
     const std::string pr = field("precision");
     c.precision = pr == "fp16x3" ? 1 : (pr == "bf16x3" ? 2 : 0);
     c.plan_us = std::atof(field("plan_us").c_str());
-    return n > 0 && valid_radices(c.radices, n) && c.row_threads >= 0 && c.row_threads <= 512;
+    // empty radices: the planner's tile shape and radix order (only the arithmetic is recorded)
+    return n > 0 && (c.radices.empty() || valid_radices(c.radices, n)) && c.row_threads >= 0 && c.row_threads <= 512;
 }
 
 }  // namespace
@@ -384,6 +386,106 @@ BatchPlan *find_batch(void *h)
 
 }  // namespace
 
+namespace {
+
+// One uneven-batch launch over every group, timed (us per launch); false if it
+// cannot be planned or run.
+bool time_mix(const std::vector<int64_t> &sizes, const std::vector<int64_t> &rows_per, bool forward, int device,
+              void *in, void *out, cudaEvent_t e0, cudaEvent_t e1, double &us)
+{
+    BatchPlan bp;
+    bp.device = device;
+    bp.forward = forward;
+    bp.sizes = sizes;
+    bp.batches = rows_per;
+    if (!build_batch(bp).empty()) {
+        cudaGetLastError();
+        return false;
+    }
+    void *ws = nullptr;
+    if (bp.ws_bytes && cudaMalloc(&ws, bp.ws_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    bool ok = true;
+    for (int rep = 0; rep < 2 && ok; rep++) ok = enqueue(bp, in, out, ws, 0) == cudaSuccess;
+    cudaEventRecord(e0, 0);
+    for (int rep = 0; rep < 4 && ok; rep++) ok = enqueue(bp, in, out, ws, 0) == cudaSuccess;
+    cudaEventRecord(e1, 0);
+    ok = ok && cudaEventSynchronize(e1) == cudaSuccess;
+    if (ws) cudaFree(ws);
+    if (!ok) {
+        cudaGetLastError();
+        return false;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    us = ms * 1e3 / 4.0;
+    return true;
+}
+
+// The per-length winners were timed one length at a time.  In the mixed
+// launch every segment shares the grid and the CTA's shared memory is sized
+// by the largest tile of any segment, so a winner's tile shape and radix
+// order are kept only if the launch of all the groups together runs faster
+// with them (lengths taken by decreasing bytes; the arithmetic choice of
+// precision mode 3 is kept either way).
+void accept_in_mix(const std::vector<int64_t> &sizes, const std::vector<int64_t> &rows_per,
+                   const std::vector<int64_t> &targets, bool forward, int device, cudaEvent_t e0, cudaEvent_t e1)
+{
+    int64_t total = 0;
+    for (size_t i = 0; i < sizes.size(); i++) total += sizes[i] * rows_per[i];
+    void *in = nullptr, *out = nullptr;
+    if (cudaMalloc(&in, total * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&out, total * sizeof(float2)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(in);
+        return;  // no room for the whole mix: the per-length winners stand
+    }
+    cudaMemset(in, 0, total * sizeof(float2));
+    // bytes of the launch whose tiles each tuned length shapes (as a group or as a pass)
+    std::map<int64_t, int64_t> weight;
+    for (size_t i = 0; i < sizes.size(); i++) {
+        if (sizes[i] <= kBatchMaxRowN) weight[sizes[i]] += sizes[i] * rows_per[i];
+        else
+            for (int r : multipass_split(sizes[i])) weight[r] += sizes[i] * rows_per[i];
+    }
+    std::vector<std::pair<int64_t, int64_t>> order;  // (bytes, length)
+    std::map<int64_t, TuneChoice> winners;
+    for (const int64_t n : targets) {
+        TuneChoice c;
+        if (!tuned_choice(n, c) || c.radices.empty()) continue;
+        winners[n] = c;
+        order.push_back({weight[n], n});
+        TuneChoice plain = c;  // the planner's defaults for the launch, the arithmetic kept
+        plain.radices.clear();
+        plain.maxe = 0;
+        plain.row_threads = 0;
+        set_tuned_choice(n, plain);
+    }
+    std::sort(order.rbegin(), order.rend());
+    double best = 0.0;
+    if (time_mix(sizes, rows_per, forward, device, in, out, e0, e1, best)) {
+        for (const auto &o : order) {
+            const TuneChoice keep = winners[o.second];
+            TuneChoice plain = keep;
+            plain.radices.clear();
+            plain.maxe = 0;
+            plain.row_threads = 0;
+            set_tuned_choice(o.second, keep);
+            double us = 0.0;
+            if (time_mix(sizes, rows_per, forward, device, in, out, e0, e1, us) && us < best * 0.995)
+                best = us;
+            else
+                set_tuned_choice(o.second, plain);
+        }
+    }
+    cudaFree(in);
+    cudaFree(out);
+}
+
+}  // namespace
+
 // Times each candidate in the uneven-batch kernel (a one-group batch plan of
 // about 4 M points of the length) and records the fastest; for lengths with a
 // tensor-core stage also times the whole ordinary plan in each arithmetic.
@@ -408,9 +510,18 @@ int autotune_lengths(const std::vector<int64_t> &sizes, const std::vector<int64_
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (size_t i = 0; i < sizes.size(); i++) {
-        const int64_t n = sizes[i];
-        if (n > 16384) continue;  // multi-pass lengths keep the planner's split
+    // The lengths whose tiles the uneven-batch kernel runs: groups of at most
+    // 16384 points, and the pass lengths of the multi-pass split of longer rows
+    // (their passes are column tiles of those lengths)
+    std::vector<int64_t> targets;
+    for (int64_t n : sizes) {
+        if (n <= 16384) targets.push_back(n);
+        if (n > kBatchMaxRowN)
+            for (int r : multipass_split(n)) targets.push_back(r);
+    }
+    std::sort(targets.begin(), targets.end());
+    targets.erase(std::unique(targets.begin(), targets.end()), targets.end());
+    for (const int64_t n : targets) {
         TuneChoice best;
         best.us = 1e30;
         // enough transforms that a launch is not just its overhead
@@ -486,10 +597,11 @@ int autotune_lengths(const std::vector<int64_t> &sizes, const std::vector<int64_
             tuned++;
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     cudaFree(buf);
     cudaFree(out);
+    accept_in_mix(sizes, rows_per, targets, forward, device, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     return tuned;
 }
 

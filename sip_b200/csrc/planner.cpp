@@ -955,6 +955,16 @@ std::string finish(Plan &p, Builder &b, bool ok)
 
 }  // namespace
 
+// Pass lengths of a multi-pass transform of length F (the split add_multipass
+// makes), empty if F cannot be split.
+std::vector<int> multipass_split(int64_t F)
+{
+    std::vector<int> passes;
+    for (int parts = 2; parts <= 6; parts++)
+        if (split_passes(F, parts, passes)) return passes;
+    return {};
+}
+
 bool valid_radices(const std::vector<int> &r, int64_t n)
 {
     int64_t prod = 1;

@@ -288,5 +288,6 @@ std::string describe_plan(const Plan &p);
 bool factor_radices(int64_t n, std::vector<int> &radices);
 // true when every radix has a codelet in the runtime engine and they multiply to n
 bool valid_radices(const std::vector<int> &r, int64_t n);
+std::vector<int> multipass_split(int64_t F);  // pass lengths of a multi-pass transform
 
 }  // namespace sipfft

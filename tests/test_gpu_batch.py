@@ -85,8 +85,13 @@ def test_autotune_cache_round_trip(cuda, tmp_path):
     assert {l["n"] for l in lines} >= {1500, 2048, 105}
     for l in lines:
         assert l["type"] == "c2c" and l["precision"] in ("fp32", "fp16x3", "bf16x3") and l["gpu"]
-        assert int(np.prod(l["radices"])) == l["n"]
-        assert l["row_threads"] in (128, 256)
+        # a per-length winner that did not speed up the launch of all groups together
+        # is recorded without a tile choice (empty radices: the planner's defaults)
+        if l["radices"]:
+            assert int(np.prod(l["radices"])) == l["n"]
+            assert l["row_threads"] in (128, 256)
+        else:
+            assert l["row_threads"] == 0
     # 2048 has tensor-core stages: the whole plan was timed in every arithmetic
     assert [l for l in lines if l["n"] == 2048][0]["plan_us"] > 0
     assert fft.tune_cache_load(path) >= 3
