@@ -270,8 +270,12 @@ private:
         std::vector<const Req *> staged;
         int64_t rows = 0;
         for (const Req &r : l.batch) {
-            const bool aligned = (reinterpret_cast<uintptr_t>(r.in) | reinterpret_cast<uintptr_t>(r.out)) % 16 == 0;
-            if (device_io_ && aligned && in_bytes(r) >= kDirectBytes) {
+            const uintptr_t i0 = reinterpret_cast<uintptr_t>(r.in), o0 = reinterpret_cast<uintptr_t>(r.out);
+            const bool aligned = (i0 | o0) % 16 == 0;
+            // a request whose output overlaps its input keeps the staged path
+            const bool disjoint = i0 + static_cast<uintptr_t>(in_bytes(r)) <= o0 ||
+                                  o0 + static_cast<uintptr_t>(out_bytes(r)) <= i0;
+            if (device_io_ && aligned && disjoint && in_bytes(r) >= kDirectBytes) {
                 std::vector<Step> steps;
                 if (!scale_steps_to_rows(*p, r.rows, steps)) return false;
                 if (execute_steps(*p, steps, r.in, r.out, l.d_ws, l.stream) != cudaSuccess) return false;

@@ -94,6 +94,36 @@ def test_poisson_driver(cuda):
     srv.close()
 
 
+def test_large_device_requests_direct_and_in_place(cuda):
+    """Device requests of 8 MB or more run on their own buffers (no staging
+    copies); one whose output is its input keeps the staged path.  Both against
+    the oracle, batched with a small staged request of the same class."""
+    import torch
+
+    srv = fft.Server(budget_bytes=8 << 30, lanes=2, max_rows=64, device_io=True)
+    n = 65536
+    work = []
+    for i, rows in enumerate((20, 3)):          # 10.5 MB (direct) and 1.6 MB (staged)
+        x = workloads.chirp_noise(n, rows, snr_db=10.0, seed=900 + i)
+        xin = torch.from_numpy(x).cuda()
+        out = torch.empty_like(xin)
+        work.append((x, xin, out))
+    x2 = workloads.chirp_noise(n, 17, snr_db=10.0, seed=950)
+    inplace = torch.from_numpy(x2).cuda()       # 8.9 MB, output over the input
+    srv.hold(True)
+    for x, xin, out in work:
+        assert srv.submit(C2C, FWD, n, x.shape[0], xin.data_ptr(), out.data_ptr()) >= 0
+    assert srv.submit(C2C, FWD, n, 17, inplace.data_ptr(), inplace.data_ptr()) >= 0
+    srv.hold(False)
+    ids, lat = srv.drain()
+    assert len(ids) == 3 and np.all(lat > 0)
+    torch.cuda.synchronize()
+    for x, _, out in work:
+        assert oracle.rel_l2(out.cpu().numpy(), oracle.c2c(x, True)) <= oracle.tolerance(n)
+    assert oracle.rel_l2(inplace.cpu().numpy(), oracle.c2c(x2, True)) <= oracle.tolerance(n)
+    srv.close()
+
+
 def test_server_rejects_bad_requests(cuda):
     srv = fft.Server(budget_bytes=1 << 30, lanes=1, max_rows=8)
     assert srv.submit(C2C, FWD, 64, 9, 16, 16) == -1      # more rows than a lane holds
