@@ -109,8 +109,11 @@ struct TcShape {
     static constexpr int A_BYTES = M * KA * 2, B_BYTES = M * KB * 2;
     static constexpr int U1 = (KA * CA * 2 * 2 > TB * n * 8) ? KA * CA * 2 * 2 : TB * n * 8;
     static constexpr int U2 = (TB * PITCH * 8 > KB * CB * 2 * 2) ? TB * PITCH * 8 : KB * CB * 2 * 2;
+    // with N1 == N2 both stages use the same DFT matrix: one copy in shared
+    // memory (16 KB less for 256 points, so four CTAs fit an SM)
+    static constexpr bool SHARED_B = N1 == N2;
     static constexpr int OFF_AA = 128;
-    static constexpr int OFF_AB = OFF_AA + 2 * A_BYTES;
+    static constexpr int OFF_AB = SHARED_B ? OFF_AA : OFF_AA + 2 * A_BYTES;
     static constexpr int OFF_U1 = OFF_AB + 2 * B_BYTES;
     static constexpr int OFF_U2 = OFF_U1 + ((U1 + 127) / 128) * 128;
     static constexpr int SMEM = OFF_U2 + ((U2 + 127) / 128) * 128;
@@ -120,8 +123,9 @@ struct TcShape {
     static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
+// 256 points: at most 128 registers, so that four CTAs (shared memory 50 KB, TMEM 128 columns each) fit an SM
 template <int N1, int N2, int TB, int FMT, bool FWD>
-__global__ void __launch_bounds__(128, 1) tc_fft_kernel(const __grid_constant__ TileDesc d, TcArgs ta)
+__global__ void __launch_bounds__(128, N1 * N2 <= 256 ? 4 : 1) tc_fft_kernel(const __grid_constant__ TileDesc d, TcArgs ta)
 {
     using S = TcShape<N1, N2, TB, FMT, FWD>;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -143,7 +147,7 @@ __global__ void __launch_bounds__(128, 1) tc_fft_kernel(const __grid_constant__ 
         uint4 *dst[4] = {reinterpret_cast<uint4 *>(aa), reinterpret_cast<uint4 *>(aa + S::A_BYTES),
                          reinterpret_cast<uint4 *>(ab), reinterpret_cast<uint4 *>(ab + S::B_BYTES)};
         const int cnt[4] = {S::A_BYTES / 16, S::A_BYTES / 16, S::B_BYTES / 16, S::B_BYTES / 16};
-        for (int m = 0; m < 4; m++)
+        for (int m = 0; m < (S::SHARED_B ? 2 : 4); m++)
             for (int i = tid; i < cnt[m]; i += blockDim.x) dst[m][i] = __ldg(src[m] + i);
     }
     if (tid == 0) {
