@@ -178,12 +178,15 @@ __global__ void __launch_bounds__(128, N1 * N2 <= 256 ? 4 : 1) tc_fft_kernel(con
         for (int i = tid; i < (TB - ntr) * S::PITCH; i += blockDim.x) xs[ntr * S::PITCH + i] = make_float2(0.f, 0.f);
         load_tile<FWD>(d, d.in, xs, o, c0, ntr);
         __syncthreads();
-        float mx = 0.f;
-        for (int i = tid; i < TB * S::n; i += blockDim.x) {
-            const float2 x = xs[(i / S::n) * S::PITCH + pad(i % S::n)];
-            mx = fmaxf(mx, fmaxf(fabsf(x.x), fabsf(x.y)));
+        float s1 = 1.f;  // the BF16 form needs no scaling (no tile maximum)
+        if constexpr (FMT == 0) {
+            float mx = 0.f;
+            for (int i = tid; i < TB * S::n; i += blockDim.x) {
+                const float2 x = xs[(i / S::n) * S::PITCH + pad(i % S::n)];
+                mx = fmaxf(mx, fmaxf(fabsf(x.x), fabsf(x.y)));
+            }
+            s1 = range_scale<FMT>(block_max(mx, red));
         }
-        const float s1 = range_scale<FMT>(block_max(mx, red));
 
         // ---- stage A operand: column j = (t, n2), K = (n1, re/im)
         for (int idx = tid; idx < S::CA * (S::KA / 8); idx += blockDim.x) {
@@ -250,7 +253,8 @@ __global__ void __launch_bounds__(128, N1 * N2 <= 256 ? 4 : 1) tc_fft_kernel(con
         }
         tc_fence_before();
         __syncthreads();
-        const float s2 = range_scale<FMT>(block_max(mx2, red));
+        float s2 = 1.f;
+        if constexpr (FMT == 0) s2 = range_scale<FMT>(block_max(mx2, red));
         // ---- stage B operand: column j' = (t, k1), K = (n2, re/im); written over the X tile
         for (int idx = tid; idx < S::CB * (S::KB / 8); idx += blockDim.x) {
             const int j = idx % S::CB, kg = idx / S::CB;
