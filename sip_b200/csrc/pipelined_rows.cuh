@@ -105,6 +105,7 @@ __device__ __forceinline__ void r2c_post_row(const float2 *work, float2 *y, int 
 template <int MAXE, bool COMPACT = false>
 struct RuntimeEngine {
     static constexpr bool kPingPong = false;
+    static constexpr bool kSingleBuffer = false;
     static constexpr int kMaxThreads = COMPACT ? 256 : 512;
     static constexpr int kMinBlocks = COMPACT ? 3 : 1;
     template <bool FWD, class Src0, class DstL>
@@ -180,15 +181,17 @@ __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
     int64_t t = blockIdx.x;
     if (t < d.num_tiles) issue(t, 0);
     for (int i = 0; t < d.num_tiles; t += gridDim.x, i++) {
-        const int b = i & 1;
+        // two buffers: the next tile streams in while this one is transformed;
+        // one buffer (Engine::kSingleBuffer): the next tile is loaded after this one
+        const int b = Engine::kSingleBuffer ? 0 : (i & 1);
         const int64_t tn = t + gridDim.x;
-        if (tn < d.num_tiles) issue(tn, b ^ 1);
+        if (!Engine::kSingleBuffer && tn < d.num_tiles) issue(tn, b ^ 1);
         // A thread whose bounded wait gave up records it and still runs the
         // tile (on whatever the buffer holds: every access stays in bounds), so
         // that every thread reaches the same barriers; the CTA leaves together
         // at the end of the iteration.
         if (tn >= d.num_tiles) pdl_launch_dependents();  // this CTA's last tile (a CTA without tiles: at exit)
-        const bool timed_out = !mbar_wait_bounded(&bars[b], (i >> 1) & 1);
+        const bool timed_out = !mbar_wait_bounded(&bars[b], Engine::kSingleBuffer ? (i & 1) : ((i >> 1) & 1));
         if (timed_out) atomicExch(err, 1);
         const int rows = tile_rows(t);
         float2 *buf = bufs + b * buf_f2;
@@ -214,6 +217,7 @@ __global__ void __launch_bounds__(Engine::kMaxThreads, Engine::kMinBlocks)
         }
         // buffer b is free for the copy issued in iteration i+1; a CTA-uniform exit after a timeout
         if (__syncthreads_or(timed_out)) return;
+        if (Engine::kSingleBuffer && tn < d.num_tiles) issue(tn, 0);
     }
 }
 

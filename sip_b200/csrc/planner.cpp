@@ -792,7 +792,9 @@ struct Builder {
         if (inner == 1) {
             // rows up to 8192 points run as one tile; longer rows as two double-buffered
             // passes, which keep ~16 columns per tile and overlap loads with compute
-            if (n <= std::min<int64_t>(kMaxSingleTileC2C, p.max_row_n)) {
+            // (up to 16384 points where a compile-time engine exists: one row per CTA)
+            if (n <= std::min<int64_t>(kMaxSingleTileC2C, p.max_row_n) ||
+                (n <= std::min<int64_t>(kMaxRowN, p.max_row_n) && find_static_kernel(n, IO_C2C))) {
                 const float2 *tw = table(n, n);
                 if (!tw) return false;
                 Addr a{0, n, 1, 0, 0};

@@ -46,7 +46,8 @@ const void *pick(const TileDesc &d, int maxe, bool forward)
 
 size_t row_kernel_smem(const TileDesc &d)
 {
-    return 128 + (d.row_bufs > 2 ? d.row_bufs : 2) * static_cast<size_t>(d.g_ns) * sizeof(float2);
+    // row_bufs: 1 (single-buffered engines), 2, or 3 (ping-pong work area); 0 reads as 2
+    return 128 + (d.row_bufs >= 1 ? d.row_bufs : 2) * static_cast<size_t>(d.g_ns) * sizeof(float2);
 }
 
 // Raises a kernel's dynamic shared-memory limit to what the SM allows next

@@ -472,6 +472,9 @@ template <class Q, int T, class PD = Pads<>, bool PP = false, int WL = 0>
 struct StaticEngine {
     static_assert(WL == 0 || (T <= 32 && 32 % T == 0), "warp-local lanes need T dividing 32");
     static constexpr bool kPingPong = PP;  // a third shared-memory buffer holds the even boundaries
+    // a 16384-point row (139 KB padded) fits shared memory once: the row kernel
+    // loads the next tile into the same buffer after the current one is done
+    static constexpr bool kSingleBuffer = Q::N >= 16384;
     static constexpr int kMaxThreads = T <= 256 ? 256 : T;
     // 3 CTAs per SM (<= 80 registers) unless a thread holds more than 16 points
     static constexpr int kMinBlocks = T <= 256 ? (Q::N / T > 16 ? 2 : 3) : 1;

@@ -95,14 +95,14 @@ StaticKernel make_entry(int io_mask = 7)
     using E = StaticEngine<Q, T, PD, PP, (T <= 32 ? (SH ? 2 : 1) : 0)>;
     static_assert(!SH || ShflLast<Q, T, 2>::ok, "no warp-shuffle last stage for this engine");
     using EDb = StaticEngine<Q, T, PD, PP>;
-    e.row_bufs = PP ? 3 : 2;
+    e.row_bufs = PP ? 3 : (E::kSingleBuffer ? 1 : 2);
     e.fn[1][0] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, true, IO_C2C>);
     e.fn[1][1] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, true, IO_R2C_PACKED>);
     e.fn[1][2] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, true, IO_C2R_PACKED>);
     e.fn[0][0] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, false, IO_C2C>);
     e.fn[0][1] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, false, IO_R2C_PACKED>);
     e.fn[0][2] = reinterpret_cast<const void *>(pipelined_rows_kernel<E, false, IO_C2R_PACKED>);
-    if constexpr (!PP) {  // the double-buffered tile kernel has no ping-pong area
+    if constexpr (!PP && Q::N <= 8192) {  // the double-buffered tile kernel: no ping-pong area, two tiles in smem
         e.db[1] = reinterpret_cast<const void *>(static_db_kernel<EDb, true>);
         e.db[0] = reinterpret_cast<const void *>(static_db_kernel<EDb, false>);
     }
@@ -129,6 +129,9 @@ const std::vector<StaticKernel> &registry()
         make_entry<Seq<16, 16, 8>, 128, Pads<1, 16, 1, 128>>(),  // 2048
         make_entry<Seq<16, 16, 16>, 256>(),     // 4096
         make_entry<Seq<16, 16, 16, 2>, 512>(),  // 8192
+        // 16384, single pass: 32 points per thread, one row per CTA, the row loaded
+        // once per tile into a single 139 KB buffer
+        make_entry<Seq<16, 16, 16, 4>, 512>(),
         // 1500, the packed half of the 3000-point real transform: R2C on a
         // radix-5 last stage of 300 butterflies, two per thread, so that the
         // post-twiddle fuses into it; C2C and C2R on 10 x 10 x 15, one

@@ -265,13 +265,16 @@ def test_stream_and_sync(cuda):
 
 
 @pytest.mark.parametrize("typ,n", [(C2C, 1024), (C2C, 4096), (R2C, 4096), (R2C, 3000), (C2R, 3000), (C2R, 4096),
-                                   (C2C, 512), (R2C, 1024), (C2R, 1024), (R2C, 256), (C2R, 128)])
+                                   (C2C, 512), (R2C, 1024), (C2R, 1024), (R2C, 256), (C2R, 128),
+                                   (C2C, 16384), (R2C, 32768), (C2R, 32768)])
 def test_pipelined_and_generic_kernels_agree(cuda, typ, n):
     """A 16-byte aligned source takes the TMA-pipelined row kernel; an 8-byte
     aligned one (offset by one element through the aclTensor offset) takes the
     generic tile kernel.  Both must give the oracle's result.  The 1024-point
     real transforms run the 512-point engine whose last radix-2 stage is
-    warp-shuffle butterflies; 128..512-point engines use warp barriers."""
+    warp-shuffle butterflies; 128..512-point engines use warp barriers; 16384
+    points (C2C, and the packed half of 32768-point real transforms) run the
+    single-buffered one-row-per-CTA engine."""
     import torch
 
     rng = np.random.default_rng(n + typ)
