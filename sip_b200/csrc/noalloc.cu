@@ -23,6 +23,7 @@
 // looks up the array's device address (cudaGetSymbolAddress) and sets the
 // kernels' shared-memory limits; make that first call before any stream
 // capture.
+#include <algorithm>
 #include <mutex>
 
 #include "../../include/asdsip_fft_ext.h"
@@ -228,8 +229,9 @@ extern "C" int32_t asdFftExecC2CNoAlloc(const void *input, void *output, int64_t
     const int64_t F = fftSize;
 
     // Front of the array: pass-0 stage table, pass-1 stage table, then the
-    // two-level table of W_F (lo: L entries, hi: ceil(F/L) entries); at most
-    // 2048 + 2048 + 1024 + 1024 entries.  The intermediate follows.
+    // two-level table of W_F (lo: L entries, hi: ceil(F/L) entries), then each
+    // pass's per-stage tables ([r-1][k] per stage, < 2048 entries a pass); at
+    // most 2048 + 2048 + 1024 + 1024 + 2 x 2048 entries.  The intermediate follows.
     const int log2l = (log2_ceil(F) + 1) / 2;
     const int64_t L = int64_t(1) << log2l;
     float2 *tw0 = base;
@@ -245,19 +247,42 @@ extern "C" int32_t asdFftExecC2CNoAlloc(const void *input, void *output, int64_t
         set_last_error("asdFftExecC2CNoAlloc: pass does not fit a tile");
         return AsdSip::ACL_ERROR_API_NOT_SUPPORT;
     }
+    float2 *stw0 = hi + (F + L - 1) / L;
+    float2 *stw1 = stw0 + stage_twiddle_count(d0.radix, d0.nstages);
+    if (stw1 + stage_twiddle_count(d1.radix, d1.nstages) > base + kNoAllocTableElems) {
+        set_last_error("asdFftExecC2CNoAlloc: twiddle tables exceed the scratch table area");
+        return AsdSip::ACL_ERROR_API_NOT_SUPPORT;
+    }
+    d0.stw = stw0;
+    d1.stw = stw1;
     cudaError_t e = fill_twiddles(tw0, p0, p0, 1, st);
     if (e == cudaSuccess) e = fill_twiddles(tw1, p1, p1, 1, st);
     if (e == cudaSuccess) e = fill_twiddles(lo, L, F, 1, st);
     if (e == cudaSuccess) e = fill_twiddles(hi, (F + L - 1) / L, F, L, st);
+    if (e == cudaSuccess) e = fill_stage_twiddles(stw0, d0.radix, d0.nstages, st);
+    if (e == cudaSuccess) e = fill_stage_twiddles(stw1, d1.radix, d1.nstages, st);
+    // each pass on the double-buffered tile kernel when two tiles fit shared
+    // memory (the next tile's copies overlap this tile's stages), else one tile at a time
+    auto run_pass = [&](TileDesc &d, int maxe, int grid) -> cudaError_t {
+        const size_t smem2 = 2 * static_cast<size_t>(d.tb) * d.pitch * sizeof(float2);
+        if (smem2 <= static_cast<size_t>(kMaxSmemBytes)) {
+            const int per_sm = kernel_blocks_per_sm(tile_db_kernel_fn(maxe, fwd), d.tb * d.tpt, smem2);
+            if (per_sm > 0) {
+                const int64_t g = std::min<int64_t>(d.num_tiles, int64_t(per_sm) * sm_count(dev));
+                return launch_tile_db(d, maxe, fwd, static_cast<int>(g), st);
+            }
+        }
+        return launch_tile(d, maxe, fwd, grid, st);
+    };
     if (e == cudaSuccess) {
         d0.in = input;
         d0.out = data;
-        e = launch_tile(d0, maxe0, fwd, grid0, st);
+        e = run_pass(d0, maxe0, grid0);
     }
     if (e == cudaSuccess) {
         d1.in = data;
         d1.out = output;
-        e = launch_tile(d1, maxe1, fwd, grid1, st);
+        e = run_pass(d1, maxe1, grid1);
     }
     if (e != cudaSuccess) {
         set_last_error(std::string("asdFftExecC2CNoAlloc: ") + cudaGetErrorString(e));
