@@ -194,7 +194,7 @@ def test_in_place_c2c(cuda):
     import torch
 
     rng = np.random.default_rng(5)
-    for n, batch in [(1024, 64), (65536, 2)]:
+    for n, batch in [(1024, 64), (16384, 3), (65536, 2)]:
         x = _rand_complex(rng, (batch, n))
         buf = torch.from_numpy(x).cuda()
         plan = fft.FftPlan([n], C2C, FWD, batch)
@@ -314,7 +314,7 @@ def test_pipelined_and_generic_kernels_agree(cuda, typ, n):
     plan.close()
 
 
-@pytest.mark.parametrize("n,batch", [(64, 33), (256, 16), (1000, 8), (4096, 4), (65536, 2)])
+@pytest.mark.parametrize("n,batch", [(64, 33), (256, 16), (1000, 8), (4096, 4), (16384, 3), (65536, 2)])
 @pytest.mark.parametrize("fwd", [FWD, INV])
 def test_complex32_c2c(cuda, n, batch, fwd):
     """complex32 (FP16 pairs) in and out of a C2C plan, FP32 arithmetic: the
