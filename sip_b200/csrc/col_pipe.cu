@@ -60,12 +60,15 @@ struct ColOut {
 
 }  // namespace
 
-template <class Q, int T, int TB, bool FWD>
+// PP: a third shared-memory buffer holds the even stage boundaries (ping-pong
+// work rows), so stage 0 scatters outside the staged tile and no stage needs a
+// barrier between its gather and its scatter.
+template <class Q, int T, int TB, bool PP, bool FWD>
 __global__ void __launch_bounds__(TB *T, (TB * T <= 256) ? 3 : 1)
     col_pipe_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ TileDesc d, int *err)
 {
     pdl_enter();
-    using E = StaticEngine<Q, T>;
+    using E = StaticEngine<Q, T, Pads<>, PP>;
     constexpr int N = Q::N;
     constexpr int BOX = N < 256 ? N : 256;
     constexpr int NBOX = N / BOX;
@@ -112,9 +115,11 @@ __global__ void __launch_bounds__(TB *T, (TB * T <= 256) ? 3 : 1)
         const int64_t left = d.n_cols - c0;
         const bool active = l < left;
         float2 *buf = bufs + b * buf_f2;
+        float2 *work2 = PP ? bufs + 2 * buf_f2 + l * d.pitch : nullptr;
         const int64_t kc = d.g_twiddle ? pass_column(d, c0 + l) : -1;
         E::template run<FWD>(d, buf + l * d.pitch, ColStage<TB, FWD>{buf, l, &d, kc},
-                             ColOut{out + col_base(d.out_a, o, c0 + l), d.out_a.estride}, false, lane, active);
+                             ColOut{out + col_base(d.out_a, o, c0 + l), d.out_a.estride}, false, lane, active,
+                             work2);
         // buffer b is free for the copy issued in iteration i+1; a CTA-uniform exit after a timeout
         if (__syncthreads_or(timed_out)) return;
     }
@@ -124,28 +129,29 @@ __global__ void __launch_bounds__(TB *T, (TB * T <= 256) ? 3 : 1)
 namespace {
 
 struct ColPipeEntry {
-    int n, tpt, tb;
-    const void *fn[2];  // [forward]
+    int n, tpt, tb, bufs;  // bufs: shared-memory buffers of col_buf float2 each (3: ping-pong work rows)
+    const void *fn[2];     // [forward]
 };
 
-template <class Q, int T, int TB>
+template <class Q, int T, int TB, bool PP = false>
 ColPipeEntry col_entry()
 {
     static_assert(TB % 2 == 0 && TB * T <= 512, "column tile shape");
-    return ColPipeEntry{Q::N, T, TB,
-                        {reinterpret_cast<const void *>(col_pipe_kernel<Q, T, TB, false>),
-                         reinterpret_cast<const void *>(col_pipe_kernel<Q, T, TB, true>)}};
+    return ColPipeEntry{Q::N, T, TB, PP ? 3 : 2,
+                        {reinterpret_cast<const void *>(col_pipe_kernel<Q, T, TB, PP, false>),
+                         reinterpret_cast<const void *>(col_pipe_kernel<Q, T, TB, PP, true>)}};
 }
 
 // Engines with 16 points per thread (the same radix sequences as the
 // power-of-two row engines); TB columns per tile as the planner chooses them
 // (CTAs of at most 256 threads, three per SM, while TB stays >= 4, i.e. rows
-// of at least one 32-byte sector; 512 threads for 2048 points).
+// of at least one 32-byte sector; 512 threads for 2048 points, one CTA per SM,
+// whose shared memory also holds the ping-pong work rows).
 const std::vector<ColPipeEntry> &col_registry()
 {
     static const std::vector<ColPipeEntry> r = {
         col_entry<Seq<16, 4>, 4, 16>(),     col_entry<Seq<16, 8>, 8, 16>(),   col_entry<Seq<16, 16>, 16, 16>(),
-        col_entry<Seq<16, 16, 2>, 32, 8>(), col_entry<Seq<16, 16, 4>, 64, 4>(), col_entry<Seq<16, 16, 8>, 128, 4>(),
+        col_entry<Seq<16, 16, 2>, 32, 8>(), col_entry<Seq<16, 16, 4>, 64, 4>(), col_entry<Seq<16, 16, 8>, 128, 4, true>(),
     };
     return r;
 }
@@ -178,6 +184,13 @@ const void *col_pipe_kernel_fn(int n, int tpt, int tb, bool forward)
     return nullptr;
 }
 
+int col_pipe_bufs(int n, int tpt, int tb)
+{
+    for (const ColPipeEntry &e : col_registry())
+        if (e.n == n && e.tpt == tpt && e.tb == tb) return e.bufs;
+    return 2;
+}
+
 bool col_pipe_has_engine(int n)
 {
     for (const ColPipeEntry &e : col_registry())
@@ -193,7 +206,10 @@ void col_pipe_kernel_fns(std::vector<const void *> &out)
     }
 }
 
-size_t col_pipe_smem(const TileDesc &d) { return 128 + 2 * static_cast<size_t>(d.col_buf) * sizeof(float2); }
+size_t col_pipe_smem(const TileDesc &d)
+{
+    return 128 + (d.row_bufs == 3 ? 3 : 2) * static_cast<size_t>(d.col_buf) * sizeof(float2);
+}
 
 bool col_pipe_layout_ok(const TileDesc &d)
 {

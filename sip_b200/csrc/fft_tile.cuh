@@ -114,8 +114,9 @@ struct TileDesc {
     int planar;
     const float *in_im;
     float *out_im;
-    // Shared-memory buffers of a row kernel, each g_ns float2: 2 (double-
-    // buffered tiles; 0 reads as 2) or 3 (plus a ping-pong work area).
+    // Shared-memory buffers of a row kernel, each g_ns float2 (of a TMA column
+    // kernel: each col_buf float2): 2 (double-buffered tiles; 0 reads as 2) or
+    // 3 (plus a ping-pong work area).
     int row_bufs;
     // complex32 (FP16 real / imaginary pairs) user data of a C2C step: bit 0 =
     // the input, bit 1 = the output.  Loads widen to FP32, the stages run in

@@ -371,6 +371,7 @@ struct Builder {
             if (cfn && col_pipe_layout_ok(d)) {
                 const int64_t need = int64_t(d.tb) * std::max(n, d.pitch);
                 d.col_buf = (need + 15) / 16 * 16;
+                d.row_bufs = col_pipe_bufs(static_cast<int>(n), d.tpt, d.tb);
                 const int cps = kernel_blocks_per_sm(cfn, d.tb * d.tpt, col_pipe_smem(d));
                 if (cps > 0) {
                     s.cp_fn = cfn;

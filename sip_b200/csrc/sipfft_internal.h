@@ -74,6 +74,7 @@ const StaticKernel *find_static_kernel(int n, int io);
 // tile must match an instantiation.
 const void *col_pipe_kernel_fn(int n, int tpt, int tb, bool forward);
 bool col_pipe_has_engine(int n);  // a TMA column engine exists for this length
+int col_pipe_bufs(int n, int tpt, int tb);  // its shared-memory tile buffers (TileDesc::row_bufs)
 void col_pipe_kernel_fns(std::vector<const void *> &out);
 size_t col_pipe_smem(const TileDesc &d);
 // the step's input addressing and sizes fit the tensor map of the column kernel
