@@ -63,7 +63,11 @@ struct ColOut {
 // PP: a third shared-memory buffer holds the even stage boundaries (ping-pong
 // work rows), so stage 0 scatters outside the staged tile and no stage needs a
 // barrier between its gather and its scatter.
-template <class Q, int T, int TB, bool PP, bool FWD>
+// COUT: each column's N outputs are contiguous (output element stride 1, the
+// first pass of a multi-pass transform): the last stage writes the work rows and
+// the CTA then stores whole column runs, a warp 32 consecutive elements instead
+// of 16 columns x 2.
+template <class Q, int T, int TB, bool PP, bool COUT, bool FWD>
 __global__ void __launch_bounds__(TB *T, (TB * T <= 256) ? 3 : 1)
     col_pipe_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ TileDesc d, int *err)
 {
@@ -80,6 +84,7 @@ __global__ void __launch_bounds__(TB *T, (TB * T <= 256) ? 3 : 1)
     const int tid = threadIdx.x;
     const int l = tid % TB, lane = tid / TB;
     float2 *out = static_cast<float2 *>(d.out);
+    __shared__ int64_t s_base[COUT ? TB : 1];  // output offsets of the tile's columns (COUT)
 
     if (tid == 0) {
         mbar_init(&bars[0], 1);
@@ -117,9 +122,22 @@ __global__ void __launch_bounds__(TB *T, (TB * T <= 256) ? 3 : 1)
         float2 *buf = bufs + b * buf_f2;
         float2 *work2 = PP ? bufs + 2 * buf_f2 + l * d.pitch : nullptr;
         const int64_t kc = d.g_twiddle ? pass_column(d, c0 + l) : -1;
-        E::template run<FWD>(d, buf + l * d.pitch, ColStage<TB, FWD>{buf, l, &d, kc},
-                             ColOut{out + col_base(d.out_a, o, c0 + l), d.out_a.estride}, false, lane, active,
-                             work2);
+        if constexpr (COUT) {
+            if (tid < TB) s_base[tid] = col_base(d.out_a, o, c0 + tid);
+            E::template run<FWD>(d, buf + l * d.pitch, ColStage<TB, FWD>{buf, l, &d, kc}, SmemRow{buf + l * d.pitch},
+                                 true, lane, active, work2);
+            __syncthreads();
+            const int cols = left < TB ? static_cast<int>(left) : TB;
+            for (int c = 0; c < cols; c++) {
+                float2 *dst = out + s_base[c];
+                const float2 *src = buf + c * d.pitch;
+                for (int e = tid; e < N; e += TB * T) st_stream(dst + e, src[pad(e)]);
+            }
+        } else {
+            E::template run<FWD>(d, buf + l * d.pitch, ColStage<TB, FWD>{buf, l, &d, kc},
+                                 ColOut{out + col_base(d.out_a, o, c0 + l), d.out_a.estride}, false, lane, active,
+                                 work2);
+        }
         // buffer b is free for the copy issued in iteration i+1; a CTA-uniform exit after a timeout
         if (__syncthreads_or(timed_out)) return;
     }
@@ -130,16 +148,24 @@ namespace {
 
 struct ColPipeEntry {
     int n, tpt, tb, bufs;  // bufs: shared-memory buffers of col_buf float2 each (3: ping-pong work rows)
-    const void *fn[2];     // [forward]
+    const void *fn[2][2];  // [contiguous column outputs][forward]
 };
 
 template <class Q, int T, int TB, bool PP = false>
 ColPipeEntry col_entry()
 {
     static_assert(TB % 2 == 0 && TB * T <= 512, "column tile shape");
-    return ColPipeEntry{Q::N, T, TB, PP ? 3 : 2,
-                        {reinterpret_cast<const void *>(col_pipe_kernel<Q, T, TB, PP, false>),
-                         reinterpret_cast<const void *>(col_pipe_kernel<Q, T, TB, PP, true>)}};
+    ColPipeEntry e{Q::N, T, TB, PP ? 3 : 2,
+                   {{reinterpret_cast<const void *>(col_pipe_kernel<Q, T, TB, PP, false, false>),
+                     reinterpret_cast<const void *>(col_pipe_kernel<Q, T, TB, PP, false, true>)},
+                    {nullptr, nullptr}}};
+    // staged contiguous-column stores pay off where a warp's direct stores would
+    // cover less than a 32-byte sector of each column (TB >= 16: two lanes, 16 bytes)
+    if constexpr (TB >= 16) {
+        e.fn[1][0] = reinterpret_cast<const void *>(col_pipe_kernel<Q, T, TB, PP, true, false>);
+        e.fn[1][1] = reinterpret_cast<const void *>(col_pipe_kernel<Q, T, TB, PP, true, true>);
+    }
+    return e;
 }
 
 // Engines with 16 points per thread (the same radix sequences as the
@@ -177,10 +203,13 @@ EncodeTiledFn encode_fn()
 
 }  // namespace
 
-const void *col_pipe_kernel_fn(int n, int tpt, int tb, bool forward)
+const void *col_pipe_kernel_fn(int n, int tpt, int tb, bool forward, bool contiguous_out)
 {
     for (const ColPipeEntry &e : col_registry())
-        if (e.n == n && e.tpt == tpt && e.tb == tb) return e.fn[forward ? 1 : 0];
+        if (e.n == n && e.tpt == tpt && e.tb == tb) {
+            const int f = forward ? 1 : 0;
+            return contiguous_out && e.fn[1][f] ? e.fn[1][f] : e.fn[0][f];
+        }
     return nullptr;
 }
 
@@ -200,10 +229,10 @@ bool col_pipe_has_engine(int n)
 
 void col_pipe_kernel_fns(std::vector<const void *> &out)
 {
-    for (const ColPipeEntry &e : col_registry()) {
-        out.push_back(e.fn[0]);
-        out.push_back(e.fn[1]);
-    }
+    for (const ColPipeEntry &e : col_registry())
+        for (int c = 0; c < 2; c++)
+            for (int f = 0; f < 2; f++)
+                if (e.fn[c][f]) out.push_back(e.fn[c][f]);
 }
 
 size_t col_pipe_smem(const TileDesc &d)

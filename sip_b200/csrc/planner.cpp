@@ -367,7 +367,8 @@ struct Builder {
             }
             // TMA column tiles of the same engine: box copies instead of per-element
             // copies, last stage stored from registers
-            const void *cfn = s.db_fn ? col_pipe_kernel_fn(n, d.tpt, d.tb, s.forward) : nullptr;
+            const void *cfn =
+                s.db_fn ? col_pipe_kernel_fn(n, d.tpt, d.tb, s.forward, d.out_a.estride == 1) : nullptr;
             if (cfn && col_pipe_layout_ok(d)) {
                 const int64_t need = int64_t(d.tb) * std::max(n, d.pitch);
                 d.col_buf = (need + 15) / 16 * 16;

@@ -71,8 +71,10 @@ struct StaticKernel {
 const StaticKernel *find_static_kernel(int n, int io);
 // TMA-pipelined column kernels (col_pipe.cu) for the power-of-two static
 // engines with 16 points per thread: n, threads per transform and columns per
-// tile must match an instantiation.
-const void *col_pipe_kernel_fn(int n, int tpt, int tb, bool forward);
+// tile must match an instantiation.  contiguous_out: each column's outputs are
+// contiguous (output element stride 1); the variant that stages them through
+// shared memory is returned where one exists.
+const void *col_pipe_kernel_fn(int n, int tpt, int tb, bool forward, bool contiguous_out);
 bool col_pipe_has_engine(int n);  // a TMA column engine exists for this length
 int col_pipe_bufs(int n, int tpt, int tb);  // its shared-memory tile buffers (TileDesc::row_bufs)
 void col_pipe_kernel_fns(std::vector<const void *> &out);
