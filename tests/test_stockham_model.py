@@ -81,3 +81,40 @@ def test_fused_r2c_last_stage(n, R, fwd):
     X = sm.fused_r2c_last_stage(Z, R, fwd)
     assert not np.isnan(X).any()
     assert oracle.rel_l2(X, oracle.r2c(x, fwd)) < 1e-12
+
+
+# TMA column-kernel instantiations (col_pipe.cu col_registry): N, threads per
+# column, columns per tile, ping-pong work rows
+COLUMN_ENGINES = [(64, 4, 16, False), (128, 8, 16, False), (256, 16, 16, False), (512, 32, 8, False),
+                  (1024, 64, 4, False), (2048, 128, 4, True)]
+
+
+def _pad(i):
+    return i + (i >> 4)
+
+
+@pytest.mark.parametrize("n,t,tb,pp", COLUMN_ENGINES)
+def test_column_kernel_buffers_and_staged_stores(n, t, tb, pp):
+    """col_pipe.cu: every shared-memory index of a column tile stays inside its
+    buffer (staged [row][TB] tile, padded work rows, the third ping-pong buffer),
+    the dynamic shared memory fits a CTA, and the staged contiguous-column
+    store (TB = 16 variants) writes each element of each column exactly once."""
+    # planner.cpp choose_cfg: the column-tile pitch (bank rule P mod 32/TB = 16/TB)
+    p = _pad(n - 1) + 1
+    m, want = 32 // tb, 16 // tb
+    while p % m != want:
+        p += 1
+    col_buf = (tb * max(n, p) + 15) // 16 * 16
+    bufs = 3 if pp else 2
+    assert 128 + bufs * col_buf * 8 <= 227 * 1024
+    assert n * tb <= col_buf  # staged tile, dense [row][TB]
+    assert (tb - 1) * p + _pad(n - 1) < col_buf  # work rows (and ping-pong rows in the third buffer)
+    if tb >= 16:
+        threads = tb * t
+        seen = np.zeros((tb, n), dtype=np.int64)
+        for tid in range(threads):
+            for c in range(tb):
+                for e in range(tid, n, threads):
+                    assert c * p + _pad(e) < col_buf
+                    seen[c, e] += 1
+        assert (seen == 1).all()
